@@ -1,0 +1,253 @@
+/*
+ * scmf.h - C ABI of the B200 single-chain-in-mean-field (SCMF) polymer Monte
+ * Carlo engine (libscmf.so).
+ *
+ * The reference (ren5885a/New_arch) has no plugin or FFI layer: its boundary is
+ * a set of blocking host C++ functions that mutate a managed-memory `Phase`
+ * struct, plus its file surface (configuration.dat, polymer.dat,
+ * density_<step>.dat, coord.dat, out.vtk).  Each entry point below names the
+ * reference function or file it replaces.
+ *
+ * Conventions
+ *   - Every function returns scmf_status: 0 = ok, negative = error; the message
+ *     of the last error on the calling thread is returned by scmf_last_error().
+ *   - Plain pointers and sizes only.  Host buffers are owned by the caller;
+ *     getters copy into them.  A system owns all of its device memory (no
+ *     managed memory).
+ *   - A system handle is not thread-safe.  The server is thread-safe for
+ *     submit and poll.
+ *   - Positions cross the ABI in the reference's AoS layout (x,y,z per bead,
+ *     beads of one chain contiguous, chains grouped by architecture in the
+ *     order they were added; init_config.cu:753, device_function.cu:104-114).
+ *   - Counts and omega are laid out [type][z][y][x] (device_function.cuh:17-20,
+ *     device_function.cu:359).
+ */
+#ifndef SCMF_H
+#define SCMF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t scmf_status;
+
+#define SCMF_OK 0
+#define SCMF_E_INVALID (-1)   /* bad argument or size */
+#define SCMF_E_CUDA (-2)      /* CUDA runtime error or no device */
+#define SCMF_E_NOMEM (-3)     /* device or host allocation failed / over budget */
+#define SCMF_E_IO (-4)        /* file could not be opened or written */
+#define SCMF_E_PARSE (-5)     /* malformed configuration.dat / polymer.dat / coord.dat */
+#define SCMF_E_STATE (-6)     /* call not allowed in the current state */
+#define SCMF_E_TIMEOUT (-7)   /* a bounded wait ran out */
+#define SCMF_E_DEVICE (-8)    /* a kernel reported an error word */
+
+#define SCMF_MAX_TYPES 8      /* monomer types */
+#define SCMF_MAX_DEGREE 8     /* bonds per bead */
+#define SCMF_MAX_LENGTH 4096  /* beads per chain */
+
+/* hamiltonian */
+#define SCMF_HAM_SCMF0 0      /* reference SCMF0, device_function.cu:373-412 */
+#define SCMF_HAM_LITERAL 1    /* omega_T = [kN (sum phi - 1) + sum_{S!=T} chiN_TS phi_S] / N_ref */
+/* field_rule */
+#define SCMF_FIELD_REFERENCE 0  /* omega not recomputed when step % 10 == 0 (test.cpp:42) */
+#define SCMF_FIELD_EVERY 1      /* omega recomputed after every sweep */
+
+const char* scmf_last_error(void);
+const char* scmf_version(void);
+
+/* ------------------------------------------------------------------ spec */
+/* A system specification: box, grid, interactions and polymer
+ * architectures.  Replaces Read_polymer_config + initialize_values
+ * (init_config.cu:210-451, 455-736) and their derived constants. */
+typedef struct scmf_spec scmf_spec;
+
+typedef struct scmf_params {
+    int32_t reference_nbeads;  /* N_ref ("Polymer length unit", init_config.cu:267) */
+    double harmonic_normb;     /* k of the harmonic bond energy k |r_i - r_j|^2 (init_config.cu:484) */
+    double smc_a;              /* smart-MC A; R = sqrt(2A) (init_config.cu:807-808) */
+    uint64_t seed;             /* Philox key */
+    int32_t hamiltonian;       /* SCMF_HAM_* */
+    int32_t field_rule;        /* SCMF_FIELD_* */
+    int32_t count_bits;        /* 32, or 16 (only when total beads < 65536) */
+    int32_t reserved;
+} scmf_params;
+
+typedef struct scmf_spec_info {
+    int64_t n_beads;
+    int64_t n_cells;
+    int32_t n_chains;
+    int32_t n_types;
+    int32_t n_arch;
+    int32_t nx, ny, nz;
+    double lx, ly, lz;
+    double field_scaling;      /* n_cells / n_beads (init_config.cu:785) */
+    double harmonic_normb, smc_a, smc_r;
+    int32_t reference_nbeads;
+    int32_t count_bits;
+} scmf_spec_info;
+
+scmf_status scmf_spec_create(int32_t n_mono_types, int32_t nx, int32_t ny, int32_t nz,
+                             double lx, double ly, double lz, scmf_spec** out);
+/* xn[t + n*s] as in Phase_info_gpu::xn (init_config.cu:670-672): diagonal
+ * kappaN, off-diagonal chiN. */
+scmf_status scmf_spec_set_xn(scmf_spec* spec, const double* xn, int32_t n);
+scmf_status scmf_spec_set_params(scmf_spec* spec, const scmf_params* p);
+/* Adds n_chains chains of one architecture: mono_type[length], bonds as
+ * n_bonds (i,j) pairs.  init_sigma <= 0 selects the reference's per-component
+ * initial bond sigma 1/sqrt(3(length-1)) (device_function.cu:169-171). */
+scmf_status scmf_spec_add_arch(scmf_spec* spec, int32_t length, int32_t n_chains,
+                               const int32_t* mono_type, int32_t n_bonds, const int32_t* bonds,
+                               double init_sigma);
+/* Reference input files: configuration.dat (init_config.cu:487-512) and
+ * polymer.dat (init_config.cu:214-340), parsed by the same literal patterns.
+ * Derived constants follow init_config.cu:480-484, 807-808. */
+scmf_status scmf_spec_load_files(const char* configuration_dat, const char* polymer_dat,
+                                 uint64_t seed, scmf_spec** out);
+scmf_status scmf_spec_get_info(const scmf_spec* spec, scmf_spec_info* out);
+scmf_status scmf_spec_get_params(const scmf_spec* spec, scmf_params* out);
+scmf_status scmf_spec_get_xn(const scmf_spec* spec, double* xn, int32_t n);
+/* Architecture idx: mono_type[length] and bonds[2*n_bonds] are copied when the
+ * capacities (in elements) suffice; length / n_bonds are always returned. */
+scmf_status scmf_spec_get_arch(const scmf_spec* spec, int32_t idx, int32_t* length, int32_t* n_chains,
+                               int32_t* mono_type, int32_t type_cap, int32_t* bonds, int32_t bond_cap,
+                               int32_t* n_bonds, double* init_sigma);
+scmf_status scmf_spec_copy(const scmf_spec* spec, scmf_spec** out);
+void scmf_spec_destroy(scmf_spec* spec);
+
+/* ---------------------------------------------------------------- system */
+typedef struct scmf_system scmf_system;
+
+typedef struct scmf_stats {
+    uint64_t step;            /* completed sweeps */
+    uint64_t last_accepts;    /* accepted moves in the last sweep */
+    uint64_t total_accepts;
+    uint64_t total_moves;
+    double e_bond;            /* sum over bonds of k |r_i - r_j|^2 after the last sweep */
+    double e_field;           /* sum_T sum_cells omega_T n_T after the last field step */
+    uint32_t error_word;      /* nonzero if a kernel flagged an error */
+    uint32_t reserved;
+} scmf_stats;
+
+/* Allocates and owns all device memory of the system (initialize_structure_GPU,
+ * init_config.cu:737-854).  cuda_stream may be NULL for a private stream. */
+scmf_status scmf_system_create(const scmf_spec* spec, void* cuda_stream, scmf_system** out);
+void scmf_system_destroy(scmf_system* sys);
+scmf_status scmf_system_get_info(const scmf_system* sys, scmf_spec_info* out);
+scmf_status scmf_system_stream(const scmf_system* sys, void** cuda_stream);
+/* Random-walk initial coordinates (initialize_coord, device_function.cu:140-207),
+ * followed by the initial grid and field (test.cpp:21-23). */
+scmf_status scmf_init_coords(scmf_system* sys);
+/* Restart from host coordinates, AoS float[3*n_beads] (Generate_init_coord with
+ * read_file=1, init_config.cu:930-987), followed by the initial grid + field. */
+scmf_status scmf_set_coords(scmf_system* sys, const float* xyz, size_t n_floats);
+scmf_status scmf_get_coords(const scmf_system* sys, float* xyz, size_t n_floats);
+scmf_status scmf_set_step(scmf_system* sys, uint64_t step);   /* -Start_time (init.cpp:33) */
+/* n_sweeps full MC steps: move -> grid -> field, the field skipped per the
+ * field rule.  Replaces the body of the loop at test.cpp:37-43. */
+scmf_status scmf_step(scmf_system* sys, int32_t n_sweeps);
+/* The same, enqueued on the system's stream without waiting (for graphs of
+ * the caller's own work and for timing with events on that stream). */
+scmf_status scmf_step_async(scmf_system* sys, int32_t n_sweeps);
+/* Reference-shaped pieces of one step (blocking, like the originals): */
+scmf_status scmf_smc_move(scmf_system* sys, int32_t n_sweeps);          /* smc_move, smc.cu:3-72 */
+scmf_status scmf_reset_density_fields(scmf_system* sys);                /* reset_density_fields, mesh.cu:161-190 */
+scmf_status scmf_update_omega_fields_scmf0(scmf_system* sys);           /* update_omega_fields_scmf0, mesh.cu:217-248 */
+scmf_status scmf_synchronize(scmf_system* sys);
+scmf_status scmf_get_counts(const scmf_system* sys, uint32_t* out, size_t n);
+scmf_status scmf_get_omega(const scmf_system* sys, float* out, size_t n);
+scmf_status scmf_set_omega(scmf_system* sys, const float* in, size_t n);
+scmf_status scmf_get_stats(const scmf_system* sys, scmf_stats* out);
+
+/* Diagnostics: evaluates the device arithmetic (Philox4x32-10 with counter
+ * (c0,c1,c2,c3) = (i, 0, 0, 0) and the given key, then log(u01(w.x)),
+ * sin/cos of the angle of w.y and the three Box-Muller normals) for i < n on
+ * the GPU, for comparison with any host restatement.  out must hold 8*n
+ * floats: 4 raw words (as bits), log, sin, cos, normal0 per i; normals[3*n]. */
+scmf_status scmf_debug_math(uint32_t key_lo, uint32_t key_hi, int32_t n, uint32_t* words, float* logs,
+                            float* sines, float* cosines, float* normals);
+
+/* --------------------------------------------------------------- output */
+/* density_<step>.dat writer (io_out_density, io.cpp:4-56).  path NULL uses the
+ * reference's file name rule in the current directory. */
+scmf_status scmf_write_density(const scmf_system* sys, const char* path, int64_t step);
+/* coord.dat writer (io_out_coord, io.cpp:95-118). */
+scmf_status scmf_write_coords(const scmf_system* sys, const char* path);
+/* coord.dat reader: skips skip_beads lines (init_config.cu:955-959), then reads
+ * n_beads "%lg %lg %lg" lines into xyz (AoS float). */
+scmf_status scmf_read_coords_file(const char* path, int64_t skip_beads, float* xyz, size_t n_floats);
+/* density file -> out.vtk STRUCTURED_POINTS of phi_0 - phi_1 (vtk.c:4-81).
+ * values_per_point = 6 reproduces vtk.c exactly (it reads six numbers per
+ * grid point whatever the type count); 0 takes 2*n_types from the file. */
+scmf_status scmf_vtk_convert(const char* density_path, const char* vtk_path, int32_t values_per_point);
+
+/* -------------------------------------------------------------- batched */
+/* Many independent systems advanced together: one persistent kernel per
+ * phase over a work list of (system, chain tile) and (system, cell tile),
+ * captured once in a CUDA graph.  No reference counterpart (the reference runs
+ * one system per process). */
+typedef struct scmf_batch scmf_batch;
+
+typedef struct scmf_tune {
+    int32_t chains_per_tile;   /* 0 = per-architecture default */
+    int32_t threads_move;      /* 0 = default */
+    int32_t cells_per_tile;    /* 0 = default */
+    int32_t threads_field;     /* 0 = default */
+    int32_t persistent_ctas;   /* 0 = one CTA per tile (no persistence) */
+    int32_t use_graph;         /* 1 = capture one sweep in a CUDA graph */
+    int32_t reserved[2];
+} scmf_tune;
+
+scmf_status scmf_batch_create(scmf_system* const* systems, int32_t n, const scmf_tune* tune,
+                              void* cuda_stream, scmf_batch** out);
+scmf_status scmf_batch_step(scmf_batch* b, int32_t n_sweeps);
+/* Times candidate tunings on snapshots of the batch's systems (their state is
+ * restored afterwards) and installs the fastest; *out receives it. */
+scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps_per_trial, scmf_tune* out);
+scmf_status scmf_batch_get_tune(const scmf_batch* b, scmf_tune* out);
+void scmf_batch_destroy(scmf_batch* b);
+/* create + step + destroy */
+scmf_status scmf_batch_run(scmf_system* const* systems, int32_t n, int32_t n_sweeps, const scmf_tune* tune);
+
+/* --------------------------------------------------------------- served */
+/* A request loop with continuous batching: requests are admitted as device
+ * memory (against hbm_budget_bytes) and slots free up, state stays resident
+ * on the device between sweeps, and requests that arrive while others run
+ * join the next round.  No reference counterpart. */
+typedef struct scmf_server scmf_server;
+
+typedef struct scmf_server_opts {
+    uint64_t hbm_budget_bytes;
+    int32_t max_active;         /* 0 = unlimited */
+    int32_t sweeps_per_round;   /* 0 = default */
+    int32_t use_graph;
+    int32_t reserved;
+} scmf_server_opts;
+
+typedef struct scmf_result {
+    uint64_t id;
+    scmf_status status;
+    int32_t n_sweeps;
+    double e_bond, e_field;
+    uint64_t accepts;
+    int64_t n_beads;
+    double t_submit, t_admit, t_done;   /* seconds on the server's monotonic clock */
+} scmf_result;
+
+scmf_status scmf_server_create(const scmf_server_opts* opts, scmf_server** out);
+/* The server copies the spec.  counts_out (optional, uint32[n_types*n_cells])
+ * must stay valid until the result has been polled. */
+scmf_status scmf_server_submit(scmf_server* s, const scmf_spec* spec, int32_t n_sweeps,
+                               uint32_t* counts_out, uint64_t* id_out);
+/* Up to max results; waits up to wait_ms for at least one. */
+scmf_status scmf_server_poll(scmf_server* s, scmf_result* out, int32_t max, int32_t* n_out, int32_t wait_ms);
+scmf_status scmf_server_pending(scmf_server* s, int32_t* queued, int32_t* active, uint64_t* bytes_in_use);
+double scmf_server_now(const scmf_server* s);
+void scmf_server_destroy(scmf_server* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCMF_H */

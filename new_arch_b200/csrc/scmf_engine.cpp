@@ -1,0 +1,340 @@
+// Host engine of libscmf: specs, systems, work plans, the plain and batched
+// step loops, and the C ABI entry points of include/scmf.h except file I/O
+// (scmf_files.cpp) and serving (scmf_server.cpp).
+//
+// The reference's host orchestration (smc.cu:3-72, mesh.cu:161-248,
+// mesh_mpi.cpp:4-27, test.cpp:37-43) launches one kernel at a time with a
+// cudaDeviceSynchronize after each and a P2P/MPI density reduction.  Here a
+// sweep is two launches on one stream (fused move+grid, then field) with no
+// host round trip, optionally replayed from a CUDA graph; the step counter,
+// the counts double buffer and the statistics live on the device.
+#include "scmf_engine.h"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <mutex>
+
+namespace scmf {
+
+static thread_local std::string g_last_error;
+
+scmf_status fail(scmf_status code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+void clear_error() { g_last_error.clear(); }
+const char* last_error_cstr() { return g_last_error.c_str(); }
+
+#define CK(expr)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (expr);                                                                   \
+        if (e_ != cudaSuccess) return fail(SCMF_E_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CKL(expr)                                                                                      \
+    do {                                                                                               \
+        int e_ = (expr);                                                                               \
+        if (e_ != 0)                                                                                   \
+            return fail(SCMF_E_CUDA, "%s: %s", #expr, cudaGetErrorString((cudaError_t)e_));          \
+    } while (0)
+
+// ceil(2^32 / n): for i * n < 2^32, i / n == umulhi(i, magic).  n == 1 has no
+// 32-bit magic; the kernels test for it.
+uint32_t magic_for(uint32_t n) {
+    if (n <= 1) return 0u;
+    return (uint32_t)((((uint64_t)1 << 32) + n - 1) / n);
+}
+
+scmf_status validate_spec(const scmf_spec& s) {
+    if (s.n_types < 1 || s.n_types > kMaxTypes) return fail(SCMF_E_INVALID, "n_mono_types %d not in [1,%d]", s.n_types, kMaxTypes);
+    if (s.nx < 1 || s.ny < 1 || s.nz < 1) return fail(SCMF_E_INVALID, "grid %d x %d x %d invalid", s.nx, s.ny, s.nz);
+    if ((int64_t)s.nx * s.ny * s.nz > ((int64_t)1 << 30)) return fail(SCMF_E_INVALID, "grid too large");
+    if (!(s.lx > 0 && s.ly > 0 && s.lz > 0)) return fail(SCMF_E_INVALID, "box lengths must be positive");
+    if ((int)s.xn.size() != s.n_types * s.n_types) return fail(SCMF_E_INVALID, "xn matrix not set");
+    if (s.p.reference_nbeads < 1) return fail(SCMF_E_INVALID, "reference_nbeads must be >= 1");
+    if (!(s.p.smc_a >= 0) || !std::isfinite(s.p.harmonic_normb)) return fail(SCMF_E_INVALID, "bad smc_a / harmonic_normb");
+    if (s.p.count_bits != 16 && s.p.count_bits != 32) return fail(SCMF_E_INVALID, "count_bits must be 16 or 32");
+    if (s.p.hamiltonian != SCMF_HAM_SCMF0 && s.p.hamiltonian != SCMF_HAM_LITERAL) return fail(SCMF_E_INVALID, "unknown hamiltonian");
+    if (s.p.field_rule != SCMF_FIELD_REFERENCE && s.p.field_rule != SCMF_FIELD_EVERY) return fail(SCMF_E_INVALID, "unknown field rule");
+    if (s.archs.empty()) return fail(SCMF_E_INVALID, "spec has no polymer architecture");
+    int64_t beads = 0, chains = 0;
+    for (const auto& a : s.archs) {
+        if (a.length < 1 || a.length > kMaxLength) return fail(SCMF_E_INVALID, "chain length %d not in [1,%d]", a.length, kMaxLength);
+        beads += (int64_t)a.length * a.n_chains;
+        chains += a.n_chains;
+    }
+    if (beads <= 0) return fail(SCMF_E_INVALID, "system has no beads");
+    if (beads >= ((int64_t)1 << 31) || chains >= ((int64_t)1 << 31)) return fail(SCMF_E_INVALID, "too many beads");
+    if (s.p.count_bits == 16 && beads >= 65536)
+        return fail(SCMF_E_INVALID, "16-bit counts need fewer than 65536 beads (%lld)", (long long)beads);
+    return SCMF_OK;
+}
+
+scmf_status prepare_archs(const scmf_spec& s, std::vector<ArchHost>* out, int64_t* n_beads, int* n_chains) {
+    out->clear();
+    int64_t nb = 0;
+    int nc = 0;
+    for (const auto& a : s.archs) {
+        ArchHost h;
+        h.length = a.length;
+        h.n_chains = a.n_chains;
+        h.chain_base = nc;
+        h.bead_base = nb;
+        h.init_sigma = (float)(a.init_sigma > 0 ? a.init_sigma : (a.length > 1 ? 1.0 / std::sqrt(3.0 * (a.length - 1.0)) : 0.0));
+        const int L = a.length;
+        h.beads.assign(L, BeadInfo{});
+        std::vector<std::vector<char>> adj(L, std::vector<char>(L, 0));
+        for (size_t b = 0; b + 1 < a.bonds.size(); b += 2) {
+            int i = a.bonds[b], j = a.bonds[b + 1];
+            if (i < 0 || j < 0 || i >= L || j >= L || i == j) return fail(SCMF_E_INVALID, "bond (%d,%d) out of range", i, j);
+            adj[i][j] = adj[j][i] = 1;
+        }
+        for (int i = 0; i < L; ++i) {
+            if (a.type[i] < 0 || a.type[i] >= s.n_types) return fail(SCMF_E_INVALID, "monomer type %d out of range", a.type[i]);
+            BeadInfo& bi = h.beads[i];
+            bi.type = (uint8_t)a.type[i];
+            int d = 0;
+            for (int j = 0; j < L; ++j)
+                if (adj[i][j]) {
+                    if (d >= kMaxDeg) return fail(SCMF_E_INVALID, "bead %d has more than %d bonds", i, kMaxDeg);
+                    bi.nbr[d++] = (uint16_t)j;
+                }
+            bi.deg = (uint8_t)d;
+            h.max_deg = std::max(h.max_deg, d);
+        }
+        // greedy colouring in index order
+        int ncol = 0;
+        for (int i = 0; i < L; ++i) {
+            unsigned used = 0;
+            for (int d = 0; d < h.beads[i].deg; ++d) {
+                int j = h.beads[i].nbr[d];
+                if (j < i) used |= 1u << h.beads[j].color;
+            }
+            int c = 0;
+            while (used & (1u << c)) ++c;
+            if (c >= kMaxColors) return fail(SCMF_E_INVALID, "architecture needs more than %d colours", kMaxColors);
+            h.beads[i].color = (uint8_t)c;
+            ncol = std::max(ncol, c + 1);
+        }
+        h.n_colors = ncol;
+        h.color_beads.clear();
+        for (int c = 0; c < ncol; ++c) {
+            h.color_off[c] = (int)h.color_beads.size();
+            for (int i = 0; i < L; ++i)
+                if (h.beads[i].color == c) h.color_beads.push_back((uint16_t)i);
+        }
+        h.color_off[ncol] = (int)h.color_beads.size();
+        nb += (int64_t)L * a.n_chains;
+        nc += a.n_chains;
+        out->push_back(std::move(h));
+    }
+    *n_beads = nb;
+    *n_chains = nc;
+    return SCMF_OK;
+}
+
+static size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+static size_t count_words(const scmf_spec& s) {
+    const size_t cells = (size_t)s.nx * s.ny * s.nz * s.n_types;
+    return s.p.count_bits == 16 ? (cells + 1) / 2 : cells;
+}
+
+size_t system_device_bytes(const scmf_spec& s) {
+    int64_t beads = 0, chains = 0, arch_bytes = 0;
+    for (const auto& a : s.archs) {
+        beads += (int64_t)a.length * a.n_chains;
+        chains += a.n_chains;
+        arch_bytes += round_up((size_t)a.length * (sizeof(BeadInfo) + 2), 256);
+    }
+    const size_t cells = (size_t)s.nx * s.ny * s.nz * s.n_types;
+    size_t b = 3 * round_up((size_t)(beads + 4) * 4, 256) + round_up((size_t)chains * 4, 256);
+    b += 2 * round_up(count_words(s) * 4, 256) + round_up(cells * 4, 256);
+    b += round_up(sizeof(SysDev), 256) + round_up(s.archs.size() * sizeof(ArchDev), 256) + arch_bytes;
+    b += (size_t)chains / 8 * sizeof(MoveTile) + 64 * 1024;  // work lists
+    return b;
+}
+
+void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d) {
+    d->n_types = s.n_types;
+    d->nx = s.nx; d->ny = s.ny; d->nz = s.nz;
+    d->n_cells = (int64_t)s.nx * s.ny * s.nz;
+    d->n_beads = n_beads;
+    // derived constants (init_config.cu:480-484, 565-567, 785, 807-808) rounded to FP32
+    d->inv_dx = (float)((double)s.nx / s.lx);
+    d->inv_dy = (float)((double)s.ny / s.ly);
+    d->inv_dz = (float)((double)s.nz / s.lz);
+    d->lx = (float)s.lx; d->ly = (float)s.ly; d->lz = (float)s.lz;
+    d->scale = (float)((double)d->n_cells / (double)n_beads);
+    d->k = (float)s.p.harmonic_normb;
+    d->k2 = (float)(2.0 * s.p.harmonic_normb);
+    d->A = (float)s.p.smc_a;
+    d->R = (float)std::sqrt(2.0 * s.p.smc_a);
+    const double inv_n = 1.0 / (double)s.p.reference_nbeads;
+    const int n = s.n_types;
+    for (int i = 0; i < kMaxTypes * kMaxTypes; ++i) d->cf[i] = 0.0f;
+    for (int t = 0; t < n; ++t)
+        for (int u = 0; u < n; ++u) {
+            const double v = s.xn[t + n * u];
+            float c;
+            if (t == u) c = (float)(v * inv_n);
+            else if (s.p.hamiltonian == SCMF_HAM_SCMF0) c = (float)(-0.5 * v * inv_n);
+            else c = (float)(v * inv_n);
+            d->cf[t + n * u] = c;
+        }
+    d->hamiltonian = s.p.hamiltonian;
+    d->field_rule = s.p.field_rule;
+    d->count16 = s.p.count_bits == 16 ? 1 : 0;
+    d->n_arch = (int)s.archs.size();
+    d->seed_lo = (uint32_t)s.p.seed;
+    d->seed_hi = (uint32_t)(s.p.seed >> 32);
+}
+
+scmf_tune default_tune() {
+    scmf_tune t{};
+    t.chains_per_tile = 0;
+    t.threads_move = 256;
+    t.cells_per_tile = 0;
+    t.threads_field = 256;
+    t.persistent_ctas = 0;
+    t.use_graph = 1;
+    return t;
+}
+
+scmf_tune resolve_tune(const scmf_tune* t) {
+    scmf_tune r = default_tune();
+    if (!t) return r;
+    if (t->chains_per_tile > 0) r.chains_per_tile = t->chains_per_tile;
+    if (t->threads_move > 0) r.threads_move = std::min(512, std::max(32, t->threads_move / 32 * 32));
+    if (t->cells_per_tile > 0) r.cells_per_tile = t->cells_per_tile;
+    if (t->threads_field > 0) r.threads_field = std::min(256, std::max(32, t->threads_field / 32 * 32));
+    r.persistent_ctas = std::max(0, t->persistent_ctas);
+    r.use_graph = t->use_graph;
+    return r;
+}
+
+
+void DevPlan::release() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (graph_src) cudaGraphDestroy(graph_src);
+    if (d_move) cudaFree(d_move);
+    if (d_field) cudaFree(d_field);
+    graph = nullptr;
+    graph_src = nullptr;
+    d_move = nullptr;
+    d_field = nullptr;
+    n_move = n_field = 0;
+}
+
+scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t) {
+    release();
+    tune = t;
+    n_move = (int)p.move.size();
+    n_field = (int)p.field.size();
+    max_tile_beads = p.max_tile_beads;
+    max_length = p.max_length;
+    n_types_uniform = p.n_types_uniform;
+    CK(cudaMalloc(&d_move, std::max<size_t>(1, p.move.size()) * sizeof(MoveTile)));
+    CK(cudaMalloc(&d_field, std::max<size_t>(1, p.field.size()) * sizeof(FieldTile)));
+    CK(cudaMemcpy(d_move, p.move.data(), p.move.size() * sizeof(MoveTile), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_field, p.field.data(), p.field.size() * sizeof(FieldTile), cudaMemcpyHostToDevice));
+    return SCMF_OK;
+}
+
+scmf_status DevPlan::enqueue_sweep(cudaStream_t st) const {
+    LaunchShape ms{tune.persistent_ctas > 0 ? std::min(tune.persistent_ctas, n_move) : 0, tune.threads_move, 0, 0};
+    CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, ms, st));
+    LaunchShape fs{tune.persistent_ctas > 0 ? std::min(tune.persistent_ctas, n_field) : 0, tune.threads_field, 0,
+                   n_types_uniform};
+    CKL(launch_field(true, 0, d_field, n_field, fs, st));
+    return SCMF_OK;
+}
+
+scmf_status DevPlan::run_sweeps(cudaStream_t st, int n) {
+    if (n <= 0) return SCMF_OK;
+    if (tune.use_graph) {
+        if (!graph) {
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            scmf_status rc = enqueue_sweep(st);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (rc != SCMF_OK) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e != cudaSuccess) return fail(SCMF_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+            graph_src = g;
+            CK(cudaGraphInstantiate(&graph, g, 0));
+        }
+        for (int i = 0; i < n; ++i) CK(cudaGraphLaunch(graph, st));
+        return SCMF_OK;
+    }
+    for (int i = 0; i < n; ++i) {
+        scmf_status rc = enqueue_sweep(st);
+        if (rc) return rc;
+    }
+    return SCMF_OK;
+}
+
+scmf_status fetch_sysdev(const scmf_system* s, SysDev* out) {
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemcpy(out, s->d_sys, sizeof(SysDev), cudaMemcpyDeviceToHost));
+    return SCMF_OK;
+}
+
+}  // namespace scmf
+
+using namespace scmf;
+
+// Work tiles of this system appended to a plan.
+scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
+    const int64_t target_small = std::max<int64_t>(1, n_beads / (2 * 148));
+    for (size_t a = 0; a < archs.size(); ++a) {
+        const ArchHost& A = archs[a];
+        if (A.n_chains == 0) continue;
+        int cpt = t.chains_per_tile;
+        if (cpt <= 0) {
+            const int64_t target = std::min<int64_t>(2048, std::max<int64_t>(A.length, target_small));
+            cpt = (int)std::max<int64_t>(1, target / A.length);
+        }
+        cpt = std::max(1, std::min(cpt, kMaxTileBeads / A.length));
+        for (int c = 0; c < A.n_chains; c += cpt) {
+            MoveTile mt;
+            mt.sys = d_sys;
+            mt.arch = d_arch + a;
+            mt.chain0 = A.chain_base + c;
+            mt.n_chains = std::min(cpt, A.n_chains - c);
+            mt.bead0 = A.bead_base + (int64_t)c * A.length;
+            p->move.push_back(mt);
+            p->max_tile_beads = std::max(p->max_tile_beads, mt.n_chains * A.length);
+        }
+        p->max_length = std::max(p->max_length, A.length);
+        p->max_deg = std::max(p->max_deg, A.max_deg);
+    }
+    int64_t cpt_cells = t.cells_per_tile;
+    if (cpt_cells <= 0) cpt_cells = std::min<int64_t>(16384, std::max<int64_t>(1024, n_cells / (2 * 148)));
+    const int ntile = (int)((n_cells + cpt_cells - 1) / cpt_cells);
+    for (int i = 0; i < ntile; ++i) {
+        FieldTile ft;
+        ft.sys = d_sys;
+        ft.cell0 = (int64_t)i * cpt_cells;
+        ft.n_cells = (int)std::min<int64_t>(cpt_cells, n_cells - ft.cell0);
+        ft.n_tiles_sys = ntile;
+        p->field.push_back(ft);
+    }
+    if (p->n_types_uniform == 0 && p->field.size() == (size_t)ntile) p->n_types_uniform = spec.n_types;
+    else if (p->n_types_uniform != spec.n_types) p->n_types_uniform = 0;
+    // round the smem tile up so float4 staging stays aligned
+    p->max_tile_beads = (p->max_tile_beads + 3) & ~3;
+    return SCMF_OK;
+}
+

@@ -1,0 +1,118 @@
+// Host-side engine objects behind the C ABI (include/scmf.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "scmf.h"
+#include "scmf_internal.h"
+
+// A system specification (box, grid, interactions, architectures).  Plain
+// host data; nothing here touches the GPU.
+struct scmf_spec {
+    int n_types = 0, nx = 0, ny = 0, nz = 0;
+    double lx = 0, ly = 0, lz = 0;
+    std::vector<double> xn;  // [t + n*s]
+    scmf_params p{};
+    struct Arch {
+        int length = 0, n_chains = 0;
+        std::vector<int> type;   // [length]
+        std::vector<int> bonds;  // pairs
+        double init_sigma = 0;   // per-component sigma of the initial random walk
+    };
+    std::vector<Arch> archs;
+};
+
+namespace scmf {
+
+scmf_status fail(scmf_status code, const char* fmt, ...);
+void clear_error();
+const char* last_error_cstr();
+
+// Architecture prepared for the device: adjacency in ascending index order,
+// greedy colouring in index order, beads grouped by colour, division magics.
+struct ArchHost {
+    int length = 0, n_colors = 0, n_chains = 0, chain_base = 0, max_deg = 0;
+    int64_t bead_base = 0;
+    float init_sigma = 0;
+    std::vector<BeadInfo> beads;
+    std::vector<uint16_t> color_beads;
+    int color_off[kMaxColors + 1] = {};
+};
+
+scmf_status validate_spec(const scmf_spec& s);
+scmf_status prepare_archs(const scmf_spec& s, std::vector<ArchHost>* out, int64_t* n_beads, int* n_chains);
+uint32_t magic_for(uint32_t n);
+size_t system_device_bytes(const scmf_spec& s);
+void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d);
+
+// Work decomposition of one or many systems for one launch shape.
+struct Plan {
+    std::vector<MoveTile> move;
+    std::vector<FieldTile> field;
+    int max_tile_beads = 0;
+    int max_length = 0;
+    int n_types_uniform = 0;
+    int max_deg = 0;
+};
+
+struct DevPlan {
+    MoveTile* d_move = nullptr;
+    FieldTile* d_field = nullptr;
+    int n_move = 0, n_field = 0;
+    int max_tile_beads = 0, max_length = 0, n_types_uniform = 0;
+    scmf_tune tune{};
+    cudaGraphExec_t graph = nullptr;
+    cudaGraph_t graph_src = nullptr;
+    void release();
+    scmf_status upload(const Plan& p, const scmf_tune& t);
+    // one fused sweep (move+grid, field) enqueued on `st`
+    scmf_status enqueue_sweep(cudaStream_t st) const;
+    scmf_status run_sweeps(cudaStream_t st, int n);
+};
+
+scmf_tune default_tune();
+scmf_tune resolve_tune(const scmf_tune* t);
+
+}  // namespace scmf
+
+struct scmf_system {
+    scmf_spec spec;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    int64_t n_beads = 0, n_cells = 0;
+    int n_chains = 0;
+    size_t device_bytes = 0;
+    // device buffers
+    float* x = nullptr;
+    float* y = nullptr;
+    float* z = nullptr;
+    uint32_t* chain_id = nullptr;
+    uint32_t* counts[2] = {nullptr, nullptr};
+    float* omega = nullptr;
+    scmf::SysDev* d_sys = nullptr;
+    scmf::ArchDev* d_arch = nullptr;
+    void* d_arch_blob = nullptr;
+    float* d_aos = nullptr;      // staging for AoS coordinate transfers (lazy)
+    uint32_t* d_u32 = nullptr;   // staging for unpacked 16-bit counts (lazy)
+    std::vector<scmf::ArchHost> archs;
+    std::vector<scmf::ArchDev> h_arch;  // host image of d_arch
+    scmf::DevPlan plan;                  // default work plan of this system alone
+
+    scmf_status append_plan(const scmf_tune& t, scmf::Plan* p);
+};
+
+struct scmf_batch {
+    std::vector<scmf_system*> systems;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    scmf::DevPlan plan;
+};
+
+namespace scmf {
+scmf_status fetch_sysdev(const scmf_system* s, SysDev* out);
+scmf_status current_counts(const scmf_system* s, uint32_t* host_out, size_t n);
+scmf_status write_density_file(const scmf_system* s, const char* path, int64_t step);
+}  // namespace scmf

@@ -1,0 +1,125 @@
+// Internal data model shared by the host engine (C++) and the kernels (CUDA).
+//
+// HBM layout of one system (all cudaMalloc'd, owned by the system):
+//   x, y, z      float[n_beads]       SoA bead coordinates, unwrapped (the box is
+//                                      folded only when a cell index is taken,
+//                                      device_function.cu:313-360).  Beads of a
+//                                      chain are contiguous; chains are grouped
+//                                      by architecture (init_config.cu:610-629).
+//   chain_id     uint32[n_chains]     storage slot -> global chain id (the RNG
+//                                      key), so chains can be reordered in space
+//                                      without changing any result.
+//   counts[2]    uint32[n_types*n_cells] (or uint16 pairs)  per-type cell counts,
+//                                      [type][z][y][x]; double-buffered so the
+//                                      fused sweep accumulates into one buffer
+//                                      while the field step clears the other.
+//   omega        float[n_types*n_cells]  quasi-instantaneous field.
+// plus a SysDev descriptor in device memory holding constants, the sweep
+// counter and the statistics accumulators.
+#pragma once
+#include <stdint.h>
+
+namespace scmf {
+
+constexpr int kMaxTypes = 8;
+constexpr int kMaxDeg = 8;
+constexpr int kMaxColors = 8;
+constexpr int kMaxLength = 4096;    // beads per chain (16-bit neighbour indices)
+constexpr int kMaxTileBeads = 8192;  // beads staged in shared memory per tile
+constexpr int kSlots = 32;           // spread of the statistics atomics
+constexpr uint32_t kInitStep = 0xFFFFFFFFu;
+
+// Per-bead architecture record.
+struct BeadInfo {
+    uint8_t type, deg, color, pad;
+    uint16_t nbr[kMaxDeg];
+};
+
+// One polymer architecture of one system.
+struct ArchDev {
+    const BeadInfo* beads;       // [length]
+    const uint16_t* color_beads; // [length], beads grouped by colour
+    int32_t length;
+    int32_t n_colors;
+    int32_t color_off[kMaxColors + 1];
+    uint32_t color_magic[kMaxColors];  // ceil(2^32 / n_in_colour): i / n == umulhi(i, magic)
+    uint32_t len_magic;          // ceil(2^32 / length)
+    int32_t n_chains;
+    int32_t chain_base;          // first global chain id of this architecture
+    int64_t bead_base;           // first bead of this architecture in the system arrays
+    float init_sigma;
+};
+
+struct SysDev {
+    float* x;
+    float* y;
+    float* z;
+    uint32_t* chain_id;
+    uint32_t* counts[2];
+    float* omega;
+    int64_t n_cells;
+    int64_t n_beads;
+    int32_t n_types, nx, ny, nz;
+    float inv_dx, inv_dy, inv_dz, scale;
+    float lx, ly, lz;
+    float k, k2, A, R;
+    float cf[kMaxTypes * kMaxTypes];
+    int32_t hamiltonian, field_rule, count16, n_arch;
+    uint32_t seed_lo, seed_hi;
+    // mutable state
+    uint32_t step;        // completed sweeps
+    uint32_t cur;         // counts[cur] holds the counts of the current positions
+    uint32_t field_done;  // field tiles finished in the current launch
+    uint32_t error_word;
+    unsigned long long slot_acc[kSlots];
+    double slot_eb[kSlots];
+    double slot_ef[kSlots];
+    // statistics of the last completed sweep
+    unsigned long long last_accepts, total_accepts, total_moves;
+    double e_bond, e_field;
+};
+
+// Work item of the move / grid kernel: a run of whole chains of one architecture.
+struct MoveTile {
+    SysDev* sys;
+    const ArchDev* arch;
+    int32_t chain0;       // first storage slot (system-wide chain index)
+    int32_t n_chains;
+    int64_t bead0;        // first bead (system arrays)
+};
+
+// Work item of the field kernel: a run of cells of one system.
+struct FieldTile {
+    SysDev* sys;
+    int64_t cell0;
+    int32_t n_cells;
+    int32_t n_tiles_sys;  // field tiles of this system in the launch
+};
+
+enum SweepMode : int { kMoveOnly = 0, kMoveGrid = 1, kGridOnly = 2 };
+
+// Launchers (scmf_kernels.cu).  Every pointer is device memory.
+struct LaunchShape {
+    int blocks;    // 0 = one CTA per tile
+    int threads;
+    int smem;      // unused by the launchers (they size shared memory themselves)
+    int n_types;   // field kernel: monomer types shared by all systems, 0 = mixed
+};
+
+int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);
+int launch_sweep(int mode, const MoveTile* tiles, int n_tiles, int max_tile_beads, int max_length,
+                 LaunchShape shape, void* stream);
+int launch_field(bool fused, int force_update, const FieldTile* tiles, int n_tiles, LaunchShape shape,
+                 void* stream);
+int launch_finalize_move(SysDev* sys, void* stream);
+int launch_aos_to_soa(const float* aos, SysDev* sys, const ArchDev* arch, int n_arch, int64_t n_beads,
+                      void* stream);
+int launch_soa_to_aos(float* aos, const SysDev* sys, const ArchDev* arch, int n_arch, int64_t n_beads,
+                      void* stream);
+int launch_unpack_counts16(const SysDev* sys, uint32_t* out, int64_t n, void* stream);
+size_t sweep_smem_bytes(int max_tile_beads, int max_length);
+int configure_kernels();
+int launch_debug_math(uint32_t k0, uint32_t k1, int n, uint32_t* words, float* logs, float* sines, float* cosines,
+                      float* normals, void* stream);
+
+}  // namespace scmf

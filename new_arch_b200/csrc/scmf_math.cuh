@@ -1,0 +1,123 @@
+// Device arithmetic of the SCMF engine: counter-based Philox4x32-10, uniform
+// and Gaussian variates, and project-written log / sin / cos.
+//
+// Every routine is IEEE single precision built from +, -, *, correctly rounded
+// division and sqrt, and explicit __fmaf_rn; the translation unit is compiled
+// with --fmad=false -prec-div=true -prec-sqrt=true so nothing else is fused.
+// The results are therefore a pure function of the inputs and identical to a
+// host build of the same expressions with -ffp-contract=off.
+//
+// The reference draws from a stateful cuRAND Philox4_32_10 per chain
+// (device_function.cu:12-24, 683, 749) seeded by time(NULL)
+// (init_config.cu:864).  Here the stream is stateless: the counter is
+// (chain, bead, step, draw) and the key is the 64-bit seed, so any bead move
+// can be replayed in any order.
+#pragma once
+#include <stdint.h>
+
+namespace scmf {
+
+// Philox4x32-10: Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11.  Round multipliers 0xD2511F53 / 0xCD9E8D57, key
+// increments 0x9E3779B9 / 0xBB67AE85.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// Odd multiples of 2^-24 in (0,1); exact in FP32.
+__device__ __forceinline__ float u01(uint32_t w) {
+    return __uint2float_rn((w >> 8) | 1u) * 0x1p-24f;
+}
+
+// log(x) for normal x > 0.  x = 2^e m with m in [sqrt(1/2), sqrt(2));
+// log m = 2 atanh(s), s = (m - 1)/(m + 1), series to s^11; e ln2 with a 12-bit
+// head of ln2 so that e * head is exact.
+__device__ __forceinline__ float log_f(float x) {
+    const uint32_t ix = __float_as_uint(x);
+    int e = (int)(ix >> 23) - 127;
+    uint32_t mb = (ix & 0x007FFFFFu) | 0x3F800000u;
+    if (mb > 0x3FB504F3u) {
+        mb -= 0x00800000u;
+        e += 1;
+    }
+    const float m = __uint_as_float(mb);
+    const float s = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
+    const float s2 = __fmul_rn(s, s);
+    float p = 0x1.745d18p-3f;
+    p = __fmaf_rn(p, s2, 0x1.c71c72p-3f);
+    p = __fmaf_rn(p, s2, 0x1.24924ap-2f);
+    p = __fmaf_rn(p, s2, 0x1.99999ap-2f);
+    p = __fmaf_rn(p, s2, 0x1.555556p-1f);
+    const float lm = __fmaf_rn(__fmul_rn(s, s2), p, __fmul_rn(2.0f, s));
+    const float fe = __int2float_rn(e);
+    return __fmaf_rn(fe, 0x1.62ep-1f, __fmaf_rn(fe, 0x1.0bfbe8p-15f, lm));
+}
+
+// sin and cos of 2 pi (2j+1) 2^-24 with j = w >> 9: the quadrant is removed in
+// integers, the remainder g in [-1/2, 1/2) quadrant goes through the Taylor
+// series of sin(pi g / 2) (to g^9) and cos(pi g / 2) (to g^10).
+__device__ __forceinline__ void sincos_turn(uint32_t w, float& s, float& c) {
+    const int32_t v = (int32_t)(((w >> 9) << 1) | 1u);
+    const int32_t qv = (v + (1 << 21)) >> 22;
+    const int32_t r = v - (qv << 22);
+    const int q = qv & 3;
+    const float g = __fmul_rn(__int2float_rn(r), 0x1p-22f);
+    const float g2 = __fmul_rn(g, g);
+    float sp = 0x1.507834p-13f;
+    sp = __fmaf_rn(sp, g2, -0x1.32d2ccp-8f);
+    sp = __fmaf_rn(sp, g2, 0x1.466bc6p-4f);
+    sp = __fmaf_rn(sp, g2, -0x1.4abbcep-1f);
+    sp = __fmaf_rn(sp, g2, 0x1.921fb6p+0f);
+    const float sa = __fmul_rn(g, sp);
+    float cp = -0x1.a6d1f2p-16f;
+    cp = __fmaf_rn(cp, g2, 0x1.e1f506p-11f);
+    cp = __fmaf_rn(cp, g2, -0x1.55d3c8p-6f);
+    cp = __fmaf_rn(cp, g2, 0x1.03c1f0p-2f);
+    cp = __fmaf_rn(cp, g2, -0x1.3bd3ccp+0f);
+    const float ca = __fmaf_rn(cp, g2, 1.0f);
+    if (q == 0) {
+        s = sa; c = ca;
+    } else if (q == 1) {
+        s = ca; c = -sa;
+    } else if (q == 2) {
+        s = -sa; c = -ca;
+    } else {
+        s = -ca; c = sa;
+    }
+}
+
+// Three standard normals from one Philox block (Box-Muller on (w.x, w.y) and
+// on (w.z, w.w), the last sine unused).
+__device__ __forceinline__ void normals3(uint4 w, float& n0, float& n1, float& n2) {
+    float s, c;
+    const float r0 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.x))));
+    sincos_turn(w.y, s, c);
+    n0 = __fmul_rn(r0, c);
+    n1 = __fmul_rn(r0, s);
+    const float r1 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.z))));
+    sincos_turn(w.w, s, c);
+    n2 = __fmul_rn(r1, c);
+}
+
+// floor(x * inv_d) mod n, in [0, n).  FP32 restatement of the periodic fold in
+// coord_to_index_unified_high (device_function.cu:313-360).
+__device__ __forceinline__ int fold(float x, float inv_d, int n) {
+    int i = __float2int_rd(__fmul_rn(x, inv_d));
+    if ((unsigned)i >= (unsigned)n) {
+        i %= n;
+        if (i < 0) i += n;
+    }
+    return i;
+}
+
+}  // namespace scmf

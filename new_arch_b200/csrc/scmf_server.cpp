@@ -1,0 +1,254 @@
+// Served form of the engine: a request loop with continuous batching.
+//
+// Requests (a system spec + a sweep count) are queued by scmf_server_submit.
+// One worker thread owns the GPU work: between rounds it admits queued
+// requests in arrival order while their device memory fits the HBM budget
+// (and the active-slot limit), creates and initialises their systems, then
+// runs one round of sweeps over every active system with the batched plan
+// (one move launch and one field launch per sweep for all of them).  Systems
+// stay resident between rounds; a system whose sweeps are done is read back
+// (counts, energies) and freed, and its memory goes to the next request.
+// Requests that arrive while others run join at the next round boundary.
+// No reference counterpart: the reference runs one system per process.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "scmf_engine.h"
+
+using namespace scmf;
+
+namespace {
+
+struct Request {
+    uint64_t id = 0;
+    scmf_spec spec;
+    int n_sweeps = 0;
+    uint32_t* counts_out = nullptr;
+    double t_submit = 0;
+    size_t bytes = 0;
+};
+
+struct Active {
+    Request req;
+    scmf_system* sys = nullptr;
+    int remaining = 0;
+    double t_admit = 0;
+};
+
+}  // namespace
+
+struct scmf_server {
+    scmf_server_opts opts{};
+    int device = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request> queue;
+    std::vector<Active> active;
+    std::deque<scmf_result> done;
+    uint64_t next_id = 1;
+    size_t bytes_in_use = 0;
+    int n_active = 0;  // mirror of active.size() for other threads
+    bool stop = false;
+    std::thread worker;
+    cudaStream_t stream = nullptr;
+    std::chrono::steady_clock::time_point t0;
+
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    void run();
+};
+
+static void finish(scmf_server* s, Active& a, scmf_status st) {
+    scmf_result r{};
+    r.id = a.req.id;
+    r.status = st;
+    r.n_sweeps = a.req.n_sweeps;
+    r.n_beads = a.sys ? a.sys->n_beads : 0;
+    r.t_submit = a.req.t_submit;
+    r.t_admit = a.t_admit;
+    if (a.sys && st == SCMF_OK) {
+        scmf_stats stats{};
+        scmf_status rc = scmf_get_stats(a.sys, &stats);
+        if (!rc && a.req.counts_out)
+            rc = scmf_get_counts(a.sys, a.req.counts_out, (size_t)a.sys->n_cells * a.sys->spec.n_types);
+        r.status = rc;
+        r.e_bond = stats.e_bond;
+        r.e_field = stats.e_field;
+        r.accepts = stats.total_accepts;
+    }
+    if (a.sys) scmf_system_destroy(a.sys);
+    a.sys = nullptr;
+    r.t_done = s->now();
+    std::lock_guard<std::mutex> g(s->mu);
+    s->bytes_in_use -= std::min(s->bytes_in_use, a.req.bytes);
+    s->done.push_back(r);
+    s->cv_done.notify_all();
+}
+
+void scmf_server::run() {
+    cudaSetDevice(device);
+    DevPlan plan;
+    bool plan_valid = false;
+    const int per_round = opts.sweeps_per_round > 0 ? opts.sweeps_per_round : 25;
+    scmf_tune tune = default_tune();
+    tune.use_graph = opts.use_graph;
+    for (;;) {
+        // admission
+        std::vector<Request> admit;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            if (active.empty() && queue.empty() && !stop)
+                cv_work.wait_for(lk, std::chrono::milliseconds(50));
+            if (stop && queue.empty() && active.empty()) break;
+            while (!queue.empty()) {
+                Request& r = queue.front();
+                const bool slot = opts.max_active <= 0 || (int)(active.size() + admit.size()) < opts.max_active;
+                if (!slot || bytes_in_use + r.bytes > opts.hbm_budget_bytes) break;
+                bytes_in_use += r.bytes;
+                admit.push_back(std::move(r));
+                queue.pop_front();
+            }
+        }
+        for (auto& r : admit) {
+            Active a;
+            a.req = std::move(r);
+            a.remaining = a.req.n_sweeps;
+            a.t_admit = now();
+            scmf_status rc = scmf_system_create(&a.req.spec, stream, &a.sys);
+            if (!rc) rc = scmf_init_coords(a.sys);
+            if (rc || a.remaining == 0) {
+                finish(this, a, rc);
+                continue;
+            }
+            active.push_back(std::move(a));
+            plan_valid = false;
+        }
+        {
+            std::lock_guard<std::mutex> g(mu);
+            n_active = (int)active.size();
+        }
+        if (active.empty()) continue;
+        // one round over all active systems
+        int round = per_round;
+        for (auto& a : active) round = std::min(round, a.remaining);
+        if (!plan_valid) {
+            Plan p;
+            for (auto& a : active) a.sys->append_plan(tune, &p);
+            scmf_status rc = plan.upload(p, tune);
+            if (rc) {
+                for (auto& a : active) finish(this, a, rc);
+                active.clear();
+                continue;
+            }
+            plan_valid = true;
+        }
+        scmf_status rc = plan.run_sweeps(stream, round);
+        if (!rc && cudaStreamSynchronize(stream) != cudaSuccess) rc = fail(SCMF_E_CUDA, "round failed");
+        std::vector<Active> keep;
+        for (auto& a : active) {
+            a.remaining -= round;
+            if (rc || a.remaining <= 0) {
+                finish(this, a, rc);
+                plan_valid = false;
+            } else {
+                keep.push_back(std::move(a));
+            }
+        }
+        active.swap(keep);
+        std::lock_guard<std::mutex> g(mu);
+        n_active = (int)active.size();
+    }
+    plan.release();
+}
+
+extern "C" {
+
+scmf_status scmf_server_create(const scmf_server_opts* opts, scmf_server** out) {
+    if (!opts || !out) return fail(SCMF_E_INVALID, "NULL argument");
+    if (opts->hbm_budget_bytes == 0) return fail(SCMF_E_INVALID, "hbm_budget_bytes must be > 0");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        return fail(SCMF_E_CUDA, "no CUDA device available");
+    }
+    scmf_server* s = new scmf_server;
+    s->opts = *opts;
+    s->t0 = std::chrono::steady_clock::now();
+    cudaGetDevice(&s->device);
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete s;
+        return fail(SCMF_E_CUDA, "cudaStreamCreate failed");
+    }
+    s->worker = std::thread([s] { s->run(); });
+    *out = s;
+    return SCMF_OK;
+}
+
+scmf_status scmf_server_submit(scmf_server* s, const scmf_spec* spec, int32_t n_sweeps, uint32_t* counts_out,
+                               uint64_t* id_out) {
+    if (!s || !spec || n_sweeps < 0) return fail(SCMF_E_INVALID, "bad arguments");
+    scmf_status rc = validate_spec(*spec);
+    if (rc) return rc;
+    Request r;
+    r.spec = *spec;
+    r.n_sweeps = n_sweeps;
+    r.counts_out = counts_out;
+    r.bytes = system_device_bytes(*spec);
+    if (r.bytes > s->opts.hbm_budget_bytes)
+        return fail(SCMF_E_NOMEM, "request needs %zu bytes, budget is %llu", r.bytes,
+                    (unsigned long long)s->opts.hbm_budget_bytes);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->stop) return fail(SCMF_E_STATE, "server is shutting down");
+    r.id = s->next_id++;
+    r.t_submit = s->now();
+    if (id_out) *id_out = r.id;
+    s->queue.push_back(std::move(r));
+    s->cv_work.notify_all();
+    return SCMF_OK;
+}
+
+scmf_status scmf_server_poll(scmf_server* s, scmf_result* out, int32_t max, int32_t* n_out, int32_t wait_ms) {
+    if (!s || !n_out || max < 0 || (max > 0 && !out)) return fail(SCMF_E_INVALID, "bad arguments");
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->done.empty() && wait_ms > 0)
+        s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [s] { return !s->done.empty(); });
+    int n = 0;
+    while (n < max && !s->done.empty()) {
+        out[n++] = s->done.front();
+        s->done.pop_front();
+    }
+    *n_out = n;
+    return SCMF_OK;
+}
+
+scmf_status scmf_server_pending(scmf_server* s, int32_t* queued, int32_t* active, uint64_t* bytes) {
+    if (!s) return fail(SCMF_E_INVALID, "NULL server");
+    std::lock_guard<std::mutex> g(s->mu);
+    if (queued) *queued = (int32_t)s->queue.size();
+    if (active) *active = (int32_t)s->n_active;
+    if (bytes) *bytes = s->bytes_in_use;
+    return SCMF_OK;
+}
+
+double scmf_server_now(const scmf_server* s) { return s ? s->now() : 0.0; }
+
+void scmf_server_destroy(scmf_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->stop = true;
+        s->cv_work.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+}  // extern "C"

@@ -1,0 +1,526 @@
+/*
+ * CPU oracle for the SCMF polymer Monte Carlo hot path.  TEST INFRASTRUCTURE
+ * ONLY: it is the checker the CUDA engine is compared against and never the
+ * thing measured or shipped.  See scmf_oracle.h for the reference file:line
+ * map.
+ *
+ * Build with -ffp-contract=off so that no multiply-add is contracted: every
+ * fused multiply-add below is an explicit fmaf() call, and the CUDA side uses
+ * the same explicit fused operations with --fmad=false.  Division and sqrtf
+ * are IEEE correctly rounded on both sides.
+ *
+ * Algorithm (one sweep at step s):
+ *   for every chain, for colour c = 0 .. n_colours-1, for every bead b of
+ *   colour c: a smart-MC (force-biased, Rossky-Doll-Friedman) trial against the
+ *   frozen omega field, with the Philox4x32-10 counter (chain, b, s, 0) for the
+ *   Gaussian displacement and (chain, b, s, 1) for the acceptance uniform.
+ *   Bonded beads never share a colour, so the result does not depend on the
+ *   order in which beads of one colour are visited, nor on chain order.
+ * The reference instead draws `length` random beads with replacement per chain
+ * (device_function.cu:747-751); the odd/even colouring is this engine's update
+ * order and is applied identically here and on the GPU.
+ */
+#include "scmf_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_MAX_TYPES 8
+#define ORC_MAX_ARCH 64
+#define ORC_MAX_DEG 8
+#define ORC_INIT_STEP 0xFFFFFFFFu
+
+/* ------------------------------------------------------------------ math */
+
+static inline uint32_t f2u(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+static inline float u2f(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).  Multipliers and Weyl
+ * constants are the published ones. */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* Uniform on the odd multiples of 2^-24 in (0,1): exact in float. */
+float orc_u01(uint32_t w) { return (float)((w >> 8) | 1u) * 0x1p-24f; }
+
+/* Natural log for normal positive floats: x = 2^e m, m in [sqrt(1/2), sqrt(2)),
+ * log m = 2 atanh(s), s = (m-1)/(m+1), odd series to s^11; e ln2 added with a
+ * two-part ln2 (12-bit head so that e*head is exact). */
+float orc_logf(float x) {
+    uint32_t ix = f2u(x);
+    int e = (int)(ix >> 23) - 127;
+    uint32_t mb = (ix & 0x007FFFFFu) | 0x3F800000u;
+    if (mb > 0x3FB504F3u) { mb -= 0x00800000u; e += 1; }
+    float m = u2f(mb);
+    float s = (m - 1.0f) / (m + 1.0f);
+    float s2 = s * s;
+    float p = 0x1.745d18p-3f;               /* 2/11 */
+    p = fmaf(p, s2, 0x1.c71c72p-3f);        /* 2/9 */
+    p = fmaf(p, s2, 0x1.24924ap-2f);        /* 2/7 */
+    p = fmaf(p, s2, 0x1.99999ap-2f);        /* 2/5 */
+    p = fmaf(p, s2, 0x1.555556p-1f);        /* 2/3 */
+    float lm = fmaf(s * s2, p, 2.0f * s);
+    float fe = (float)e;
+    return fmaf(fe, 0x1.62ep-1f, fmaf(fe, 0x1.0bfbe8p-15f, lm));
+}
+
+/* sin and cos of the angle 2*pi*(2j+1)*2^-24, j = w >> 9.  The quadrant is
+ * split off in integers, the remainder g in [-1/2, 1/2) of a quadrant goes
+ * through the Taylor series of sin(pi g/2) (to g^9) and cos(pi g/2) (to g^10). */
+void orc_sincos_turn(uint32_t w, float* s, float* c) {
+    int32_t v = (int32_t)(((w >> 9) << 1) | 1u);
+    int32_t qv = (v + (1 << 21)) >> 22;
+    int32_t r = v - (qv << 22);
+    int q = qv & 3;
+    float g = (float)r * 0x1p-22f;
+    float g2 = g * g;
+    float sp = 0x1.507834p-13f;
+    sp = fmaf(sp, g2, -0x1.32d2ccp-8f);
+    sp = fmaf(sp, g2, 0x1.466bc6p-4f);
+    sp = fmaf(sp, g2, -0x1.4abbcep-1f);
+    sp = fmaf(sp, g2, 0x1.921fb6p+0f);
+    float sa = g * sp;
+    float cp = -0x1.a6d1f2p-16f;
+    cp = fmaf(cp, g2, 0x1.e1f506p-11f);
+    cp = fmaf(cp, g2, -0x1.55d3c8p-6f);
+    cp = fmaf(cp, g2, 0x1.03c1f0p-2f);
+    cp = fmaf(cp, g2, -0x1.3bd3ccp+0f);
+    float ca = fmaf(cp, g2, 1.0f);
+    switch (q) {
+        case 0: *s = sa; *c = ca; break;
+        case 1: *s = ca; *c = -sa; break;
+        case 2: *s = -sa; *c = -ca; break;
+        default: *s = -ca; *c = sa; break;
+    }
+}
+
+/* Three standard normals from one Philox block: Box-Muller on (w0,w1) gives
+ * n0 = r cos, n1 = r sin; on (w2,w3) gives n2 = r cos (the fourth is unused,
+ * as curand_normal4's w is unused in device_function.cu:683-688). */
+void orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2) {
+    float s, c;
+    float r0 = sqrtf(-2.0f * orc_logf(orc_u01(w[0])));
+    orc_sincos_turn(w[1], &s, &c);
+    *n0 = r0 * c;
+    *n1 = r0 * s;
+    float r1 = sqrtf(-2.0f * orc_logf(orc_u01(w[2])));
+    orc_sincos_turn(w[3], &s, &c);
+    *n2 = r1 * c;
+}
+
+/* Periodic fold of one coordinate to a cell index in [0, n): floor(x/dx) mod n.
+ * Restates coord_to_index_unified_high (device_function.cu:313-360) in FP32. */
+int orc_fold(float x, float inv_d, int n) {
+    float t = x * inv_d;
+    int i = (int)floorf(t);
+    if ((unsigned)i >= (unsigned)n) {
+        i %= n;
+        if (i < 0) i += n;
+    }
+    return i;
+}
+
+/* ---------------------------------------------------------------- system */
+
+typedef struct orc_arch {
+    int length, n_chains, n_colors, chain_base;
+    int64_t bead_base;
+    float init_sigma;
+    int* type;          /* [length] */
+    int* deg;           /* [length] */
+    int* nbr;           /* [length * ORC_MAX_DEG], ascending */
+    int* color;         /* [length] */
+} orc_arch;
+
+struct orc_system {
+    int n_types, nx, ny, nz;
+    double lx, ly, lz;
+    double xn[ORC_MAX_TYPES * ORC_MAX_TYPES];
+    int nref;
+    double kd, ad;
+    uint64_t seed;
+    int hamiltonian, field_rule;
+    int n_arch;
+    orc_arch arch[ORC_MAX_ARCH];
+    int n_chains;
+    int64_t n_beads, n_cells;
+    /* derived float constants */
+    float k, k2, A, R, inv_dx, inv_dy, inv_dz, scale, flx, fly, flz;
+    float cf[ORC_MAX_TYPES * ORC_MAX_TYPES];
+    /* state */
+    float *x, *y, *z;
+    uint32_t* counts;
+    float* omega;
+    double* chain_ebond;
+    uint32_t* chain_acc;
+    uint64_t step;
+    orc_stats st;
+    int finalized;
+};
+
+static int g_threads = 1;
+void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+int orc_get_threads(void) { return g_threads; }
+
+orc_system* orc_create(int n_types, int nx, int ny, int nz, double lx, double ly, double lz,
+                       const double* xn, int nref, double harmonic_normb, double smc_a,
+                       uint64_t seed, int hamiltonian, int field_rule) {
+    if (n_types < 1 || n_types > ORC_MAX_TYPES || nx < 1 || ny < 1 || nz < 1) return NULL;
+    orc_system* s = (orc_system*)calloc(1, sizeof(orc_system));
+    s->n_types = n_types; s->nx = nx; s->ny = ny; s->nz = nz;
+    s->lx = lx; s->ly = ly; s->lz = lz;
+    memcpy(s->xn, xn, sizeof(double) * n_types * n_types);
+    s->nref = nref; s->kd = harmonic_normb; s->ad = smc_a; s->seed = seed;
+    s->hamiltonian = hamiltonian; s->field_rule = field_rule;
+    return s;
+}
+
+int orc_add_arch(orc_system* s, int length, int n_chains, const int* mono_type,
+                 int n_bonds, const int* bonds, double init_sigma) {
+    if (s->finalized || s->n_arch >= ORC_MAX_ARCH || length < 1 || n_chains < 0) return -1;
+    orc_arch* a = &s->arch[s->n_arch];
+    a->length = length; a->n_chains = n_chains; a->init_sigma = (float)init_sigma;
+    a->type = (int*)calloc(length, sizeof(int));
+    a->deg = (int*)calloc(length, sizeof(int));
+    a->nbr = (int*)calloc((size_t)length * ORC_MAX_DEG, sizeof(int));
+    a->color = (int*)calloc(length, sizeof(int));
+    for (int i = 0; i < length; ++i) {
+        if (mono_type[i] < 0 || mono_type[i] >= s->n_types) return -1;
+        a->type[i] = mono_type[i];
+    }
+    /* adjacency lists in ascending index order, as conection_list is built by
+     * scanning the connection matrix (init_config.cu:312-336) */
+    char* adj = (char*)calloc((size_t)length * length, 1);
+    for (int b = 0; b < n_bonds; ++b) {
+        int i = bonds[2 * b], j = bonds[2 * b + 1];
+        if (i < 0 || j < 0 || i >= length || j >= length || i == j) { free(adj); return -1; }
+        adj[(size_t)i * length + j] = adj[(size_t)j * length + i] = 1;
+    }
+    for (int i = 0; i < length; ++i)
+        for (int j = 0; j < length; ++j)
+            if (adj[(size_t)i * length + j]) {
+                if (a->deg[i] >= ORC_MAX_DEG) { free(adj); return -1; }
+                a->nbr[i * ORC_MAX_DEG + a->deg[i]++] = j;
+            }
+    free(adj);
+    /* greedy colouring in index order: smallest colour unused by lower neighbours */
+    a->n_colors = 0;
+    for (int i = 0; i < length; ++i) {
+        int used = 0;
+        for (int d = 0; d < a->deg[i]; ++d) {
+            int j = a->nbr[i * ORC_MAX_DEG + d];
+            if (j < i) used |= 1 << a->color[j];
+        }
+        int c = 0;
+        while (used & (1 << c)) ++c;
+        a->color[i] = c;
+        if (c + 1 > a->n_colors) a->n_colors = c + 1;
+    }
+    s->n_arch++;
+    return 0;
+}
+
+int orc_finalize(orc_system* s) {
+    if (s->finalized) return 0;
+    int64_t nb = 0; int nc = 0;
+    for (int a = 0; a < s->n_arch; ++a) {
+        s->arch[a].bead_base = nb;
+        s->arch[a].chain_base = nc;
+        nb += (int64_t)s->arch[a].length * s->arch[a].n_chains;
+        nc += s->arch[a].n_chains;
+    }
+    s->n_beads = nb; s->n_chains = nc;
+    s->n_cells = (int64_t)s->nx * s->ny * s->nz;
+    /* derived constants (init_config.cu:480-484, 785, 807-808), rounded to FP32 */
+    s->k = (float)s->kd;
+    s->k2 = (float)(2.0 * s->kd);
+    s->A = (float)s->ad;
+    s->R = (float)sqrt(2.0 * s->ad);
+    s->inv_dx = (float)((double)s->nx / s->lx);
+    s->inv_dy = (float)((double)s->ny / s->ly);
+    s->inv_dz = (float)((double)s->nz / s->lz);
+    s->flx = (float)s->lx; s->fly = (float)s->ly; s->flz = (float)s->lz;
+    s->scale = nb > 0 ? (float)((double)s->n_cells / (double)nb) : 0.0f;
+    double inv_n = 1.0 / (double)s->nref;
+    int n = s->n_types;
+    for (int t = 0; t < n; ++t)
+        for (int u = 0; u < n; ++u) {
+            double v = s->xn[t + n * u];
+            if (t == u) s->cf[t + n * u] = (float)(v * inv_n);
+            else if (s->hamiltonian == 0) s->cf[t + n * u] = (float)(-0.5 * v * inv_n);
+            else s->cf[t + n * u] = (float)(v * inv_n);
+        }
+    s->x = (float*)calloc(nb > 0 ? nb : 1, sizeof(float));
+    s->y = (float*)calloc(nb > 0 ? nb : 1, sizeof(float));
+    s->z = (float*)calloc(nb > 0 ? nb : 1, sizeof(float));
+    s->counts = (uint32_t*)calloc(s->n_cells * n, sizeof(uint32_t));
+    s->omega = (float*)calloc(s->n_cells * n, sizeof(float));
+    s->chain_ebond = (double*)calloc(nc > 0 ? nc : 1, sizeof(double));
+    s->chain_acc = (uint32_t*)calloc(nc > 0 ? nc : 1, sizeof(uint32_t));
+    s->finalized = 1;
+    return 0;
+}
+
+void orc_destroy(orc_system* s) {
+    if (!s) return;
+    for (int a = 0; a < s->n_arch; ++a) {
+        free(s->arch[a].type); free(s->arch[a].deg); free(s->arch[a].nbr); free(s->arch[a].color);
+    }
+    free(s->x); free(s->y); free(s->z); free(s->counts); free(s->omega);
+    free(s->chain_ebond); free(s->chain_acc);
+    free(s);
+}
+
+int64_t orc_n_beads(const orc_system* s) { return s->n_beads; }
+int64_t orc_n_cells(const orc_system* s) { return s->n_cells; }
+int orc_n_chains(const orc_system* s) { return s->n_chains; }
+void orc_set_step(orc_system* s, uint64_t step) { s->step = step; s->st.step = step; }
+
+void orc_set_coords(orc_system* s, const float* p) {
+    for (int64_t i = 0; i < s->n_beads; ++i) { s->x[i] = p[3 * i]; s->y[i] = p[3 * i + 1]; s->z[i] = p[3 * i + 2]; }
+}
+void orc_get_coords(const orc_system* s, float* p) {
+    for (int64_t i = 0; i < s->n_beads; ++i) { p[3 * i] = s->x[i]; p[3 * i + 1] = s->y[i]; p[3 * i + 2] = s->z[i]; }
+}
+void orc_get_counts(const orc_system* s, uint32_t* out) { memcpy(out, s->counts, sizeof(uint32_t) * s->n_cells * s->n_types); }
+void orc_get_omega(const orc_system* s, float* out) { memcpy(out, s->omega, sizeof(float) * s->n_cells * s->n_types); }
+void orc_set_omega(orc_system* s, const float* in) { memcpy(s->omega, in, sizeof(float) * s->n_cells * s->n_types); }
+void orc_get_stats(const orc_system* s, orc_stats* out) { *out = s->st; out->step = s->step; }
+
+static inline void key_of(const orc_system* s, uint32_t key[2]) {
+    key[0] = (uint32_t)s->seed; key[1] = (uint32_t)(s->seed >> 32);
+}
+
+/* Random-walk chains (device_function.cu:140-207): first bead uniform in the
+ * box, then every bead i in index order places each not-yet-placed neighbour
+ * at pos[i] + sigma * N(0,1)^3. */
+static void init_chain(orc_system* s, const orc_arch* a, int ci, const uint32_t key[2], char* placed) {
+    uint32_t gc = (uint32_t)(a->chain_base + ci);
+    int64_t b0 = a->bead_base + (int64_t)ci * a->length;
+    float* X = s->x + b0; float* Y = s->y + b0; float* Z = s->z + b0;
+    uint32_t ctr[4] = {gc, 0u, ORC_INIT_STEP, 0u}, w[4];
+    for (int i = 0; i < a->length; ++i) { X[i] = 0.0f; Y[i] = 0.0f; Z[i] = 0.0f; placed[i] = 0; }
+    orc_philox4x32_10(ctr, key, w);
+    X[0] = orc_u01(w[0]) * s->flx;
+    Y[0] = orc_u01(w[1]) * s->fly;
+    Z[0] = orc_u01(w[2]) * s->flz;
+    placed[0] = 1;
+    for (int i = 0; i < a->length; ++i) {
+        for (int d = 0; d < a->deg[i]; ++d) {
+            int j = a->nbr[i * ORC_MAX_DEG + d];
+            if (placed[j]) continue;
+            uint32_t c2[4] = {gc, (uint32_t)j, ORC_INIT_STEP, 1u};
+            float n0, n1, n2;
+            orc_philox4x32_10(c2, key, w);
+            orc_normals3(w, &n0, &n1, &n2);
+            X[j] = X[i] + a->init_sigma * n0;
+            Y[j] = Y[i] + a->init_sigma * n1;
+            Z[j] = Z[i] + a->init_sigma * n2;
+            placed[j] = 1;
+        }
+    }
+}
+
+void orc_init_coords(orc_system* s) {
+    uint32_t key[2]; key_of(s, key);
+    for (int a = 0; a < s->n_arch; ++a) {
+        const orc_arch* ar = &s->arch[a];
+        #pragma omp parallel num_threads(g_threads)
+        {
+            char* placed = (char*)malloc(ar->length);
+            #pragma omp for schedule(static)
+            for (int c = 0; c < ar->n_chains; ++c) init_chain(s, ar, c, key, placed);
+            free(placed);
+        }
+    }
+}
+
+static inline int64_t cell_of(const orc_system* s, float x, float y, float z) {
+    int ix = orc_fold(x, s->inv_dx, s->nx);
+    int iy = orc_fold(y, s->inv_dy, s->ny);
+    int iz = orc_fold(z, s->inv_dz, s->nz);
+    return (int64_t)ix + (int64_t)s->nx * ((int64_t)iy + (int64_t)s->ny * iz);
+}
+
+/* One smart-MC trial of bead b (device_function.cu:637-717, 562-588, 444-454). */
+static inline int move_bead(const orc_system* s, const orc_arch* a, uint32_t gc, int b,
+                            float* X, float* Y, float* Z, const uint32_t key[2], uint32_t step) {
+    const int* nb = a->nbr + b * ORC_MAX_DEG;
+    const int deg = a->deg[b];
+    const float k = s->k, k2 = s->k2, A = s->A, R = s->R;
+    float x = X[b], y = Y[b], z = Z[b];
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    for (int d = 0; d < deg; ++d) {
+        int j = nb[d];
+        fx = fx + (X[j] - x) * k2;
+        fy = fy + (Y[j] - y) * k2;
+        fz = fz + (Z[j] - z) * k2;
+    }
+    uint32_t ctr[4] = {gc, (uint32_t)b, step, 0u}, w[4];
+    orc_philox4x32_10(ctr, key, w);
+    float n0, n1, n2;
+    orc_normals3(w, &n0, &n1, &n2);
+    float dx = A * fx + R * n0;
+    float dy = A * fy + R * n1;
+    float dz = A * fz + R * n2;
+    float px = x + dx, py = y + dy, pz = z + dz;
+    float nfx = 0.0f, nfy = 0.0f, nfz = 0.0f;
+    float deb = 0.0f;
+    for (int d = 0; d < deg; ++d) {
+        int j = nb[d];
+        float qx = X[j], qy = Y[j], qz = Z[j];
+        nfx = nfx + (qx - px) * k2;
+        nfy = nfy + (qy - py) * k2;
+        nfz = nfz + (qz - pz) * k2;
+        float ox = x - qx, oy = y - qy, oz = z - qz;
+        float ex = ox + dx, ey = oy + dy, ez = oz + dz;
+        float o2 = ox * ox + oy * oy + oz * oz;
+        float e2 = ex * ex + ey * ey + ez * ez;
+        deb = deb + k * (e2 - o2);
+    }
+    float smc = 0.5f * ((nfx + fx) * dx + (nfy + fy) * dy + (nfz + fz) * dz)
+              + 0.25f * A * (nfx * nfx + nfy * nfy + nfz * nfz - fx * fx - fy * fy - fz * fz);
+    const int t = a->type[b];
+    const float* W = s->omega + (int64_t)t * s->n_cells;
+    float w_old = W[cell_of(s, x, y, z)];
+    float w_new = W[cell_of(s, px, py, pz)];
+    float dE = (w_new - w_old) + deb;
+    dE = dE + smc;
+    int acc;
+    if (dE < 0.0f) {
+        acc = 1;
+    } else {
+        uint32_t c2[4] = {gc, (uint32_t)b, step, 1u};
+        orc_philox4x32_10(c2, key, w);
+        acc = orc_logf(orc_u01(w[0])) < -dE;
+    }
+    if (acc) { X[b] = px; Y[b] = py; Z[b] = pz; }
+    return acc;
+}
+
+static double chain_bond_energy(const orc_system* s, const orc_arch* a, const float* X, const float* Y, const float* Z) {
+    double e = 0.0;
+    for (int i = 0; i < a->length; ++i)
+        for (int d = 0; d < a->deg[i]; ++d) {
+            int j = a->nbr[i * ORC_MAX_DEG + d];
+            if (j <= i) continue;
+            float ex = X[i] - X[j], ey = Y[i] - Y[j], ez = Z[i] - Z[j];
+            float r2 = ex * ex + ey * ey + ez * ez;
+            e += (double)s->k * (double)r2;
+        }
+    return e;
+}
+
+static void sweep_moves(orc_system* s, uint32_t step) {
+    uint32_t key[2]; key_of(s, key);
+    for (int a = 0; a < s->n_arch; ++a) {
+        const orc_arch* ar = &s->arch[a];
+        #pragma omp parallel for schedule(static) num_threads(g_threads)
+        for (int c = 0; c < ar->n_chains; ++c) {
+            int64_t b0 = ar->bead_base + (int64_t)c * ar->length;
+            float* X = s->x + b0; float* Y = s->y + b0; float* Z = s->z + b0;
+            uint32_t gc = (uint32_t)(ar->chain_base + c);
+            uint32_t nacc = 0;
+            for (int col = 0; col < ar->n_colors; ++col)
+                for (int b = 0; b < ar->length; ++b)
+                    if (ar->color[b] == col) nacc += (uint32_t)move_bead(s, ar, gc, b, X, Y, Z, key, step);
+            s->chain_acc[ar->chain_base + c] = nacc;
+            s->chain_ebond[ar->chain_base + c] = chain_bond_energy(s, ar, X, Y, Z);
+        }
+    }
+    uint64_t acc = 0; double eb = 0.0;
+    for (int c = 0; c < s->n_chains; ++c) { acc += s->chain_acc[c]; eb += s->chain_ebond[c]; }
+    s->st.last_accepts = acc;
+    s->st.total_accepts += acc;
+    s->st.total_moves += (uint64_t)s->n_beads;
+    s->st.e_bond = eb;
+}
+
+void orc_smc_move(orc_system* s, int n) {
+    for (int i = 0; i < n; ++i) {
+        s->step += 1;
+        sweep_moves(s, (uint32_t)s->step);
+    }
+}
+
+/* Integer per-type cell counts (device_function.cu:471-508). */
+void orc_reset_density(orc_system* s) {
+    const int64_t nc = s->n_cells;
+    memset(s->counts, 0, sizeof(uint32_t) * nc * s->n_types);
+    for (int a = 0; a < s->n_arch; ++a) {
+        const orc_arch* ar = &s->arch[a];
+        #pragma omp parallel for schedule(static) num_threads(g_threads)
+        for (int c = 0; c < ar->n_chains; ++c) {
+            int64_t b0 = ar->bead_base + (int64_t)c * ar->length;
+            for (int b = 0; b < ar->length; ++b) {
+                int64_t cell = cell_of(s, s->x[b0 + b], s->y[b0 + b], s->z[b0 + b]);
+                uint32_t* slot = &s->counts[(int64_t)ar->type[b] * nc + cell];
+                if (g_threads > 1) __atomic_fetch_add(slot, 1u, __ATOMIC_RELAXED);
+                else *slot += 1u;
+            }
+        }
+    }
+}
+
+/* SCMF0 field (device_function.cu:373-412) in FP32, or the literal
+ * omega_T = kappaN (sum phi - 1) + sum_{S!=T} chiN_TS phi_S per 1/N_ref
+ * when hamiltonian == 1. */
+static void field_update(orc_system* s, int write_omega) {
+    const int n = s->n_types;
+    const int64_t nc = s->n_cells;
+    double ef = 0.0;
+    #pragma omp parallel for schedule(static) reduction(+:ef) num_threads(g_threads)
+    for (int64_t c = 0; c < nc; ++c) {
+        float phi[ORC_MAX_TYPES];
+        float tot = 0.0f;
+        for (int u = 0; u < n; ++u) { phi[u] = (float)s->counts[u * nc + c] * s->scale; tot = tot + phi[u]; }
+        for (int t = 0; t < n; ++t) {
+            float w;
+            if (write_omega) {
+                w = (tot - 1.0f) * s->cf[t + n * t];
+                for (int u = 0; u < n; ++u) {
+                    if (u == t) continue;
+                    if (s->hamiltonian == 0) w = w + s->cf[t + n * u] * (phi[t] - phi[u]);
+                    else w = w + s->cf[t + n * u] * phi[u];
+                }
+                s->omega[t * nc + c] = w;
+            } else {
+                w = s->omega[t * nc + c];
+            }
+            ef += (double)w * (double)s->counts[t * nc + c];
+        }
+    }
+    s->st.e_field = ef;
+}
+
+void orc_update_omega(orc_system* s) { field_update(s, 1); }
+
+/* One MC step per sweep, test.cpp:37-43: move, grid, then the field unless
+ * the rule is "reference" and step % 10 == 0. */
+void orc_step(orc_system* s, int n) {
+    for (int i = 0; i < n; ++i) {
+        s->step += 1;
+        sweep_moves(s, (uint32_t)s->step);
+        orc_reset_density(s);
+        int upd = (s->field_rule == 1) || (s->step % 10 != 0);
+        field_update(s, upd);
+    }
+}

@@ -1,0 +1,176 @@
+"""GPU parity: the CUDA engine (through the C ABI) against the CPU oracle.
+
+Bead positions and density counts must be bit-identical; omega, energies
+within 1e-6 relative.  Sizes are chosen so the single-threaded oracle finishes
+in seconds."""
+import numpy as np
+import pytest
+
+from tests._util import (assert_close, assert_coords_equal, assert_counts_equal, compare_state, oracle_for)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def nb():
+    import new_arch_b200
+    return new_arch_b200
+
+
+def test_device_math_matches_oracle(nb):
+    from new_arch_b200.system import debug_math
+    from oracle import oracle as orc
+    n = 1 << 16
+    key = (0x12345678, 0x9abcdef0)
+    words, logs, s, c, normals = debug_math(n, key)
+    idx = np.random.default_rng(0).integers(0, n, 2000)
+    for i in idx:
+        w = orc.philox((int(i), 0, 0, 0), key)
+        assert np.array_equal(words[i], w)
+        assert np.float32(logs[i]).view(np.uint32) == np.float32(orc.logf(orc.lib().orc_u01(int(w[0])))).view(np.uint32)
+        so, co = orc.sincos_turn(int(w[1]))
+        assert np.float32(s[i]).view(np.uint32) == np.float32(so).view(np.uint32)
+        assert np.float32(c[i]).view(np.uint32) == np.float32(co).view(np.uint32)
+        assert np.array_equal(np.asarray(normals[i], np.float32).view(np.uint32),
+                              np.asarray(orc.normals3(w), np.float32).view(np.uint32))
+    # statistical sanity of the device normals
+    assert abs(float(normals.mean())) < 0.01
+    assert abs(float(normals.std()) - 1.0) < 0.01
+
+
+def test_init_grid_field(nb):
+    spec = nb.spec.diblock_melt(300, 32, 0.5, (8, 8, 8), 20.0, 50.0, seed=42)
+    with nb.System(spec) as s:
+        s.init_coords()
+        orc = oracle_for(spec)
+        compare_state(s, orc, "init")
+        assert int(s.counts().sum()) == spec.n_beads
+
+
+@pytest.mark.parametrize("rule", [0, 1])
+def test_steps_bit_exact(nb, rule):
+    spec = nb.spec.diblock_melt(250, 32, 0.3, (8, 10, 12), 25.0, 50.0, seed=7, field_rule=rule)
+    with nb.System(spec) as s:
+        s.init_coords()
+        orc = oracle_for(spec)
+        for chunk in (1, 4, 7):      # crosses a step % 10 == 0 boundary
+            s.step(chunk)
+            orc.step(chunk)
+            compare_state(s, orc, f"rule{rule} after {chunk}")
+
+
+def test_reference_shaped_calls(nb):
+    """smc_move -> reset_density_fields -> update_omega_fields_scmf0, as test.cpp:39-43."""
+    spec = nb.spec.diblock_melt(120, 16, 0.5, (6, 6, 6), 15.0, 50.0, seed=3, field_rule=0)
+    with nb.System(spec) as s:
+        s.init_coords()
+        orc = oracle_for(spec)
+        for step in range(1, 13):
+            s.smc_move(1)
+            orc.smc_move(1)
+            s.reset_density_fields()
+            orc.reset_density()
+            if step % 10:
+                s.update_omega_fields_scmf0()
+                orc.update_omega()
+            compare_state(s, orc, f"reference step {step}", energies=False)
+
+
+def test_blend_mixed_lengths(nb):
+    spec = nb.spec.blend_system(seed=11, n_chains=400, grid=(10, 10, 6))
+    with nb.System(spec) as s:
+        s.init_coords()
+        orc = oracle_for(spec)
+        s.step(6)
+        orc.step(6)
+        compare_state(s, orc, "blend")
+
+
+def test_branched_three_types_literal_field(nb):
+    """A comb with side chains (greedy colouring), three monomer types, the
+    literal field and 16-bit counts."""
+    from new_arch_b200.spec import Arch, SystemSpec, interaction_matrix
+    backbone = 12
+    mono = [0] * backbone
+    bonds = [[i, i + 1] for i in range(backbone - 1)]
+    for j in range(0, backbone, 3):       # side chains of two beads at every third backbone bead
+        a = len(mono)
+        mono += [1, 2]
+        bonds += [[j, a], [a, a + 1]]
+    L = len(mono)
+    spec = SystemSpec(3, 7, 6, 5, 7.0, 6.0, 5.0, interaction_matrix(3, 12.0, 40.0), 20, 3.0 / (2 * 0.49), 0.3,
+                      seed=99, hamiltonian=1, field_rule=1, count_bits=16,
+                      archs=[Arch(L, 60, mono, bonds, 0.7 / np.sqrt(3.0)),
+                             Arch(8, 25, [2] * 8, [[i, i + 1] for i in range(7)], 0.5)])
+    with nb.System(spec) as s:
+        s.init_coords()
+        orc = oracle_for(spec)
+        compare_state(s, orc, "comb init")
+        s.step(5)
+        orc.step(5)
+        compare_state(s, orc, "comb")
+
+
+def test_set_coords_restart(nb):
+    spec = nb.spec.diblock_melt(100, 24, 0.5, (6, 6, 6), 20.0, 50.0, seed=5)
+    rng = np.random.default_rng(1)
+    xyz = (rng.random((spec.n_beads, 3)) * 6.0 - 3.0).astype(np.float32)  # includes negative, unwrapped values
+    from oracle.oracle import OracleSystem
+    with nb.System(spec) as s:
+        s.set_coords(xyz)
+        s.set_step(40)
+        orc = OracleSystem(spec)
+        orc.set_coords(xyz)
+        orc.set_step(40)
+        orc.reset_density()
+        orc.update_omega()
+        assert_coords_equal(s.coords(), xyz, "round trip")
+        s.step(3)
+        orc.step(3)
+        compare_state(s, orc, "restart")
+
+
+def test_batch_bit_identical_to_alone(nb):
+    specs = nb.spec.batched_mix(6, mix_seed=5, edge_scale=0.25)
+    alone, batched = [], []
+    for sp in specs:
+        a = nb.System(sp)
+        a.init_coords()
+        a.step(5)
+        alone.append((a.coords(), a.counts(), a.omega(), a.stats()))
+        a.close()
+    systems = [nb.System(sp) for sp in specs]
+    for s in systems:
+        s.init_coords()
+    b = nb.Batch(systems, tune={"chains_per_tile": 7, "threads_move": 128, "persistent_ctas": 3})
+    b.step(2)
+    b.step(3)
+    for s, (xyz, cnt, om, st) in zip(systems, alone):
+        assert_coords_equal(s.coords(), xyz, "batched coords")
+        assert_counts_equal(s.counts(), cnt, "batched counts")
+        assert np.array_equal(s.omega(), om)
+        g = s.stats()
+        assert g["step"] == st["step"] == 5
+        assert g["total_accepts"] == st["total_accepts"]
+        assert_close([g["e_bond"]], [st["e_bond"]])
+    b.close()
+    for s in systems:
+        s.close()
+
+
+def test_autotune_keeps_state(nb):
+    specs = nb.spec.batched_mix(3, mix_seed=9, edge_scale=0.25)
+    systems = [nb.System(sp) for sp in specs]
+    for s in systems:
+        s.init_coords()
+    before = [(s.coords(), s.counts(), s.stats()["step"]) for s in systems]
+    b = nb.Batch(systems)
+    t = b.autotune(1)
+    assert t["threads_move"] in (128, 256, 512)
+    for s, (xyz, cnt, st) in zip(systems, before):
+        assert_coords_equal(s.coords(), xyz, "autotune restore")
+        assert np.array_equal(s.counts(), cnt)
+        assert s.stats()["step"] == st
+    b.close()
+    for s in systems:
+        s.close()
