@@ -1,0 +1,373 @@
+#!/usr/bin/env python3
+"""Benchmark of the SCMF polymer Monte Carlo hot path (move -> grid -> field).
+
+Metric: MC bead-moves/s (beads x sweeps / time) on one B200.  A step is one MC
+sweep of the large single system: 1.6M AB diblock chains of N=32 (51.2M
+beads), f_A=0.3, 128^3 cells, chiN=25, kappaN=50, Philox seed 7, FP32 SoA
+coordinates (614 MB, larger than L2, so no flush is needed), uint32 counts,
+FP32 omega.  Inputs are synthetic (random-walk chains).  Beside it the line
+carries the batched and served forms (256-system mix; Poisson request stream),
+the roofline of the dominant kernel, an end-to-end number through the C ABI
+with host buffers, and the CPU oracle (OpenMP) on this host's cores.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun every rank runs its own replica (the path is one system per
+GPU; replicas only), timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "MC bead-moves/s on 1 B200, batched/served vs plain; p50/p99 request latency"
+UNIT = "bead-moves/s"
+WORKLOAD = "large single system: 1.6M AB diblocks N=32 (51.2M beads), f_A=0.3, 128^3 cells, chiN=25, kappaN=50, seed 7"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--forms", choices=["all", "plain"], default="all")
+    ap.add_argument("--batched-sweeps", type=int, default=100)
+    ap.add_argument("--served-requests", type=int, default=2000)
+    ap.add_argument("--served-rate", type=float, default=200.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples SM clock and clock-event reasons through NVML in a thread."""
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+               0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+               0x100: "display_clock_setting"}
+
+    def __init__(self, local_index: int):
+        self.samples, self.reasons = [], 0
+        self._stop = threading.Event()
+        self._t = None
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = local_index
+            if vis:
+                parts = [p for p in vis.split(",") if p.strip()]
+                if local_index < len(parts) and parts[local_index].strip().isdigit():
+                    idx = int(parts[local_index])
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: report nothing rather than guess
+            self._nv = None
+            self.error = str(e)
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                    nv.nvmlDeviceGetCurrentClocksThrottleReasons
+                self.reasons |= get(self._h)
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def start(self):
+        if self._nv is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+
+    def stop(self) -> dict:
+        if self._t is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        self._stop.set()
+        self._t.join()
+        reasons = [n for b, n in self.REASONS.items() if self.reasons & b]
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": reasons, "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- helpers
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(key: str):
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(key)
+    except Exception:
+        return None
+
+
+def oracle_cpu_rate(spec, seconds: float, threads: int, warm: int = 1):
+    """Bead-moves/s of the OpenMP oracle on this host: full sweeps of `spec`."""
+    from oracle.oracle import OracleSystem, set_threads
+    set_threads(threads)
+    o = OracleSystem(spec)
+    o.init_coords()
+    o.reset_density()
+    o.update_omega()
+    o.step(warm)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        o.step(1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return spec.n_beads * n / el, n, el
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle.oracle import OracleSystem, set_threads
+    from new_arch_b200.spec import large_system
+    threads = os.cpu_count() or 1
+    set_threads(threads)
+    spec = large_system(seed=7)
+    o = OracleSystem(spec)
+    o.init_coords()
+    o.reset_density()
+    o.update_omega()
+    # each step is one full sweep of the 51.2M-bead system; if the host is so
+    # slow that K+W sweeps would exceed ~3 minutes, steps become bounded samples
+    t0 = time.perf_counter()
+    o.step(1)
+    per = time.perf_counter() - t0
+    budget = 180.0
+    sweeps_per_step = 1
+    sample = "one full sweep of the 51.2M-bead system per step"
+    if per * (args.steps + args.warmup) > budget:
+        sample = "first sweeps only (host too slow for K full sweeps)"
+    for _ in range(max(0, args.warmup - 1)):
+        o.step(1)
+    done, t0 = 0, time.perf_counter()
+    for _ in range(args.steps):
+        o.step(sweeps_per_step)
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    value = spec.n_beads * done / el
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": "host threads", "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import new_arch_b200 as nb
+    from new_arch_b200.spec import batched_mix, large_system, served_request
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- plain large system: the headline step
+    spec = large_system(seed=7 + rank)
+    s = nb.System(spec)
+    s.init_coords()
+    s.step(args.warmup)
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    s.synchronize()
+    sampler.start()
+    ms_move, ms_field, ms_total = s.step_profiled(args.steps)
+    clocks = sampler.stop()
+    barrier()
+    ms_total = allmax(ms_total)
+    st = s.stats()
+    accept_ratio = st["last_accepts"] / spec.n_beads
+    value = world * spec.n_beads * args.steps / (ms_total / 1e3)
+    peak, peak_kind = measured_peaks()
+    alg_bytes = 24 * spec.n_beads + 4 * spec.n_types * spec.n_cells          # move+grid kernel per launch
+    achieved = alg_bytes / (ms_move / args.steps / 1e3) / 1e9
+    traffic = profiled_traffic("sweep_large_system")
+    field_bytes = 12 * spec.n_types * spec.n_cells                          # read new counts, write omega, clear old counts
+    field_gbs = field_bytes / (ms_field / args.steps / 1e3) / 1e9
+
+    # ---- end to end through the C ABI with host buffers
+    xyz = s.coords()
+    pinned = torch.empty(xyz.size, dtype=torch.float32, pin_memory=True)
+    pinned.numpy()[:] = xyz.reshape(-1)
+    host_in = pinned.numpy()
+    barrier()
+    t0 = time.perf_counter()
+    s.set_coords(host_in)
+    for _ in range(args.steps):
+        s.step(1)
+        s.stats()
+    cnt = s.counts()
+    e2e_s = allmax(time.perf_counter() - t0)
+    e2e = {"value": world * spec.n_beads * args.steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": xyz.nbytes / args.steps,
+           "d2h_bytes_per_step": (64 * args.steps + cnt.nbytes) / args.steps,
+           "how": "wall clock around scmf_set_coords(pinned host xyz) + K x (scmf_step(1) + scmf_get_stats) + scmf_get_counts"}
+    s.close()
+    del pinned
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (random-walk chains)",
+            "config": {"workload": WORKLOAD, "beads": spec.n_beads, "cells": spec.n_cells, "sweeps_timed": args.steps,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (614 MB coordinates), no flush"},
+            "clocks": clocks, "e2e": e2e, "gpu_launches": 2 * args.steps,
+            "accept_ratio": accept_ratio,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "kernel": "k_sweep<move+grid>",
+                         "alg_bytes_per_launch": alg_bytes,
+                         "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+                         "ms_per_launch": ms_move / args.steps},
+            "phases": {"move_grid_ms": ms_move / args.steps, "field_ms": ms_field / args.steps,
+                       "field_gbs": field_gbs, "field_frac": field_gbs / peak}}
+
+    # ---- batched vs plain on the same 256-system mix (rank-local)
+    if args.forms == "all":
+        line["batched"] = run_batched(nb, batched_mix, args, torch)
+        line["served"] = run_served(nb, served_request, args)
+
+    # ---- CPU oracle on this host (rank 0, N=1 only)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, el = oracle_cpu_rate(spec, args.cpu_seconds, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{n} full sweeps of the 51.2M-bead system in {el:.1f} s (OpenMP oracle)"}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batched(nb, batched_mix, args, torch):
+    specs = batched_mix(256)
+    st = torch.cuda.Stream()
+    systems = [nb.System(sp, stream=st.cuda_stream) for sp in specs]
+    for x in systems:
+        x.init_coords()
+    beads = sum(sp.n_beads for sp in specs)
+    K = args.batched_sweeps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # plain engine: one system at a time, each with its own graph-launched sweeps
+    for x in systems:
+        x.step_async(1)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for x in systems:
+        x.step_async(K)
+    e1.record(st)
+    e1.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    b = nb.Batch(systems, stream=st.cuda_stream)
+    tune = b.autotune(2)
+    b.step_async(1)
+    torch.cuda.synchronize()
+    e0.record(st)
+    b.step_async(K)
+    e1.record(st)
+    e1.synchronize()
+    batched_ms = e0.elapsed_time(e1)
+    b.close()
+    for x in systems:
+        x.close()
+    plain = beads * K / (plain_ms / 1e3)
+    batched = beads * K / (batched_ms / 1e3)
+    return {"workload": "256 diblock systems, edges {16..64}^3, N {16..64}, 100 sweeps each", "beads": beads,
+            "sweeps": K, "plain_bead_moves_per_s": plain, "batched_bead_moves_per_s": batched,
+            "batched_over_plain": batched / plain, "tune": tune, "gpu_launches_batched": 2 * K,
+            "gpu_launches_plain": 2 * K * len(specs)}
+
+
+def run_served(nb, served_request, args):
+    from new_arch_b200.server import Server
+    rng = np.random.default_rng(4242)
+    n = args.served_requests
+    reqs = [served_request(rng, seed=50_000 + i) for i in range(n)]
+    gaps = rng.exponential(1.0 / args.served_rate, n)
+    arrive = np.cumsum(gaps)
+    done = []
+    with Server(150 * 10**9) as srv:
+        t0 = time.perf_counter()
+        for i, (sp, k) in enumerate(reqs):
+            now = time.perf_counter() - t0
+            if arrive[i] > now:
+                time.sleep(arrive[i] - now)
+            srv.submit(sp, k, want_counts=False)
+            done += srv.poll(256, 0)
+        while len(done) < n:
+            done += srv.poll(256, 200)
+        wall = time.perf_counter() - t0
+    lat = np.array([r["t_done"] - r["t_submit"] for r in done])
+    ok = sum(1 for r in done if r["status"] == 0)
+    moves = sum(r["n_beads"] * r["n_sweeps"] for r in done)
+    span = max(r["t_done"] for r in done) - min(r["t_submit"] for r in done)
+    return {"workload": f"Poisson {args.served_rate:g}/s, {n} requests, edges log-U[16,128], K {{50,100,500}}, 150 GB budget",
+            "requests": n, "ok": ok, "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)), "bead_moves_per_s": moves / span,
+            "offered_bead_moves_per_s": moves / float(arrive[-1]), "wall_s": wall}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -151,6 +151,12 @@ scmf_status scmf_step(scmf_system* sys, int32_t n_sweeps);
 /* The same, enqueued on the system's stream without waiting (for graphs of
  * the caller's own work and for timing with events on that stream). */
 scmf_status scmf_step_async(scmf_system* sys, int32_t n_sweeps);
+/* n_sweeps full MC steps enqueued kernel by kernel (no graph) with CUDA
+ * events around every launch on the system's stream; returns after the last
+ * sweep with the summed device time of the fused move+grid kernel, of the
+ * field kernel, and the device time from the first launch to the end of the
+ * last (milliseconds).  Same results as scmf_step. */
+scmf_status scmf_step_profiled(scmf_system* sys, int32_t n_sweeps, float* ms_move, float* ms_field, float* ms_total);
 /* Reference-shaped pieces of one step (blocking, like the originals): */
 scmf_status scmf_smc_move(scmf_system* sys, int32_t n_sweeps);          /* smc_move, smc.cu:3-72 */
 scmf_status scmf_reset_density_fields(scmf_system* sys);                /* reset_density_fields, mesh.cu:161-190 */
@@ -203,6 +209,8 @@ typedef struct scmf_tune {
 scmf_status scmf_batch_create(scmf_system* const* systems, int32_t n, const scmf_tune* tune,
                               void* cuda_stream, scmf_batch** out);
 scmf_status scmf_batch_step(scmf_batch* b, int32_t n_sweeps);
+/* The same, enqueued on the batch's stream without waiting. */
+scmf_status scmf_batch_step_async(scmf_batch* b, int32_t n_sweeps);
 /* Times candidate tunings on snapshots of the batch's systems (their state is
  * restored afterwards) and installs the fastest; *out receives it. */
 scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps_per_trial, scmf_tune* out);

@@ -93,6 +93,7 @@ SIGNATURES = {
     "scmf_set_step": (_i32, [_vp, _u64]),
     "scmf_step": (_i32, [_vp, _i32]),
     "scmf_step_async": (_i32, [_vp, _i32]),
+    "scmf_step_profiled": (_i32, [_vp, _i32, _pf32, _pf32, _pf32]),
     "scmf_smc_move": (_i32, [_vp, _i32]),
     "scmf_reset_density_fields": (_i32, [_vp]),
     "scmf_update_omega_fields_scmf0": (_i32, [_vp]),
@@ -108,6 +109,7 @@ SIGNATURES = {
     "scmf_vtk_convert": (_i32, [C.c_char_p, C.c_char_p, _i32]),
     "scmf_batch_create": (_i32, [_pvp, _i32, C.POINTER(Tune), _vp, _pvp]),
     "scmf_batch_step": (_i32, [_vp, _i32]),
+    "scmf_batch_step_async": (_i32, [_vp, _i32]),
     "scmf_batch_autotune": (_i32, [_vp, _i32, C.POINTER(Tune)]),
     "scmf_batch_get_tune": (_i32, [_vp, C.POINTER(Tune)]),
     "scmf_batch_destroy": (None, [_vp]),

@@ -67,14 +67,16 @@ scmf_status regrid(scmf_system* s) {
     CK(cudaMemsetAsync(s->counts[0], 0, counts_bytes(s), s->stream));
     CK(cudaMemsetAsync(s->counts[1], 0, counts_bytes(s), s->stream));
     CK(cudaMemsetAsync((char*)s->d_sys + offsetof(SysDev, cur), 0, sizeof(uint32_t), s->stream));
-    LaunchShape sh{0, s->plan.tune.threads_move, 0, 0};
+    LaunchShape sh = s->plan.move_shape();
+    sh.blocks = 0;
     CKL(launch_sweep(kGridOnly, s->plan.d_move, s->plan.n_move, s->plan.max_tile_beads, s->plan.max_length, sh,
                      s->stream));
     return SCMF_OK;
 }
 
 scmf_status field_now(scmf_system* s) {
-    LaunchShape sh{0, s->plan.tune.threads_field, 0, s->spec.n_types};
+    LaunchShape sh = s->plan.field_shape();
+    sh.blocks = 0;
     CKL(launch_field(false, 1, s->plan.d_field, s->plan.n_field, sh, s->stream));
     return SCMF_OK;
 }
@@ -398,9 +400,45 @@ scmf_status scmf_step(scmf_system* s, int32_t n) {
     return check_error_word(s);
 }
 
+scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float* ms_field, float* ms_total) {
+    if (!s || n < 0 || !ms_move || !ms_field || !ms_total) return fail(SCMF_E_INVALID, "bad argument");
+    *ms_move = 0.0f;
+    *ms_field = 0.0f;
+    *ms_total = 0.0f;
+    if (n == 0) return SCMF_OK;
+    std::vector<cudaEvent_t> ev(3 * (size_t)n, nullptr);
+    scmf_status rc = SCMF_OK;
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) rc = fail(SCMF_E_CUDA, "cudaEventCreate failed");
+    const DevPlan& p = s->plan;
+    const LaunchShape ms = p.move_shape();
+    const LaunchShape fs = p.field_shape();
+    for (int i = 0; i < n && !rc; ++i) {
+        cudaEventRecord(ev[3 * i], s->stream);
+        int e = launch_sweep(kMoveGrid, p.d_move, p.n_move, p.max_tile_beads, p.max_length, ms, s->stream);
+        cudaEventRecord(ev[3 * i + 1], s->stream);
+        if (!e) e = launch_field(true, 0, p.d_field, p.n_field, fs, s->stream);
+        cudaEventRecord(ev[3 * i + 2], s->stream);
+        if (e) rc = fail(SCMF_E_CUDA, "launch: %s", cudaGetErrorString((cudaError_t)e));
+    }
+    if (!rc && cudaStreamSynchronize(s->stream) != cudaSuccess) rc = fail(SCMF_E_CUDA, "sweep failed");
+    for (int i = 0; i < n && !rc; ++i) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]);
+        cudaEventElapsedTime(&b, ev[3 * i + 1], ev[3 * i + 2]);
+        *ms_move += a;
+        *ms_field += b;
+    }
+    if (!rc) cudaEventElapsedTime(ms_total, ev[0], ev[3 * (size_t)n - 1]);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (rc) return rc;
+    return check_error_word(s);
+}
+
 scmf_status scmf_smc_move(scmf_system* s, int32_t n) {
     if (!s || n < 0) return fail(SCMF_E_INVALID, "bad argument");
-    LaunchShape sh{0, s->plan.tune.threads_move, 0, 0};
+    const LaunchShape sh = s->plan.move_shape();
     for (int i = 0; i < n; ++i) {
         CKL(launch_sweep(kMoveOnly, s->plan.d_move, s->plan.n_move, s->plan.max_tile_beads, s->plan.max_length, sh,
                          s->stream));
@@ -528,10 +566,15 @@ static scmf_status batch_sync_members(scmf_batch* b) {
     return SCMF_OK;
 }
 
-scmf_status scmf_batch_step(scmf_batch* b, int32_t n) {
+scmf_status scmf_batch_step_async(scmf_batch* b, int32_t n) {
     if (!b || n < 0) return fail(SCMF_E_INVALID, "bad argument");
-    RET(batch_sync_members(b));
-    RET(b->plan.run_sweeps(b->stream, n));
+    for (auto* s : b->systems)
+        if (s->stream != b->stream) CK(cudaStreamSynchronize(s->stream));
+    return b->plan.run_sweeps(b->stream, n);
+}
+
+scmf_status scmf_batch_step(scmf_batch* b, int32_t n) {
+    RET(scmf_batch_step_async(b, n));
     CK(cudaStreamSynchronize(b->stream));
     return SCMF_OK;
 }
@@ -642,7 +685,7 @@ scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps, scmf_tune* out) {
     float best_ms = 1e30f;
     if (!rc) {
         const int tile_beads[] = {512, 1024, 2048, 4096};
-        const int threads[] = {128, 256, 512};
+        const int threads[] = {64, 128, 256};
         const int persist[] = {0, 148 * 4};
         for (int tb : tile_beads)
             for (int th : threads)

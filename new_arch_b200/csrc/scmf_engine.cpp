@@ -126,6 +126,14 @@ scmf_status prepare_archs(const scmf_spec& s, std::vector<ArchHost>* out, int64_
             ncol = std::max(ncol, c + 1);
         }
         h.n_colors = ncol;
+        h.linear = true;
+        for (int i = 0; i < L && h.linear; ++i) {
+            const BeadInfo& bi = h.beads[i];
+            const int want = (i > 0) + (i + 1 < L);
+            if (bi.deg != want || bi.color != (i & 1)) h.linear = false;
+            if (bi.deg >= 1 && i > 0 && bi.nbr[0] != i - 1) h.linear = false;
+            if (i + 1 < L && bi.nbr[bi.deg - 1] != i + 1) h.linear = false;
+        }
         h.color_beads.clear();
         for (int c = 0; c < ncol; ++c) {
             h.color_off[c] = (int)h.color_beads.size();
@@ -214,7 +222,7 @@ scmf_tune resolve_tune(const scmf_tune* t) {
     scmf_tune r = default_tune();
     if (!t) return r;
     if (t->chains_per_tile > 0) r.chains_per_tile = t->chains_per_tile;
-    if (t->threads_move > 0) r.threads_move = std::min(512, std::max(32, t->threads_move / 32 * 32));
+    if (t->threads_move > 0) r.threads_move = std::min(256, std::max(32, t->threads_move / 32 * 32));
     if (t->cells_per_tile > 0) r.cells_per_tile = t->cells_per_tile;
     if (t->threads_field > 0) r.threads_field = std::min(256, std::max(32, t->threads_field / 32 * 32));
     r.persistent_ctas = std::max(0, t->persistent_ctas);
@@ -243,6 +251,7 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t) {
     max_tile_beads = p.max_tile_beads;
     max_length = p.max_length;
     n_types_uniform = p.n_types_uniform;
+    linear = p.linear;
     CK(cudaMalloc(&d_move, std::max<size_t>(1, p.move.size()) * sizeof(MoveTile)));
     CK(cudaMalloc(&d_field, std::max<size_t>(1, p.field.size()) * sizeof(FieldTile)));
     CK(cudaMemcpy(d_move, p.move.data(), p.move.size() * sizeof(MoveTile), cudaMemcpyHostToDevice));
@@ -250,12 +259,27 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t) {
     return SCMF_OK;
 }
 
+LaunchShape DevPlan::move_shape() const {
+    LaunchShape sh{};
+    sh.blocks = tune.persistent_ctas > 0 ? std::min(tune.persistent_ctas, n_move) : 0;
+    sh.threads = tune.threads_move;
+    sh.n_types = n_types_uniform;
+    sh.linear = linear ? 1 : 0;
+    return sh;
+}
+
+LaunchShape DevPlan::field_shape() const {
+    LaunchShape sh{};
+    sh.blocks = tune.persistent_ctas > 0 ? std::min(tune.persistent_ctas, n_field) : 0;
+    sh.threads = tune.threads_field;
+    sh.n_types = n_types_uniform;
+    sh.linear = linear ? 1 : 0;
+    return sh;
+}
+
 scmf_status DevPlan::enqueue_sweep(cudaStream_t st) const {
-    LaunchShape ms{tune.persistent_ctas > 0 ? std::min(tune.persistent_ctas, n_move) : 0, tune.threads_move, 0, 0};
-    CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, ms, st));
-    LaunchShape fs{tune.persistent_ctas > 0 ? std::min(tune.persistent_ctas, n_field) : 0, tune.threads_field, 0,
-                   n_types_uniform};
-    CKL(launch_field(true, 0, d_field, n_field, fs, st));
+    CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, move_shape(), st));
+    CKL(launch_field(true, 0, d_field, n_field, field_shape(), st));
     return SCMF_OK;
 }
 
@@ -319,6 +343,7 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
         }
         p->max_length = std::max(p->max_length, A.length);
         p->max_deg = std::max(p->max_deg, A.max_deg);
+        p->linear = p->linear && A.linear;
     }
     int64_t cpt_cells = t.cells_per_tile;
     if (cpt_cells <= 0) cpt_cells = std::min<int64_t>(16384, std::max<int64_t>(1024, n_cells / (2 * 148)));

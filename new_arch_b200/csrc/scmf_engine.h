@@ -34,6 +34,7 @@ const char* last_error_cstr();
 // greedy colouring in index order, beads grouped by colour, division magics.
 struct ArchHost {
     int length = 0, n_colors = 0, n_chains = 0, chain_base = 0, max_deg = 0;
+    bool linear = false;  // bonds exactly (i, i+1): even/odd colouring, computed neighbours
     int64_t bead_base = 0;
     float init_sigma = 0;
     std::vector<BeadInfo> beads;
@@ -55,6 +56,7 @@ struct Plan {
     int max_length = 0;
     int n_types_uniform = 0;
     int max_deg = 0;
+    bool linear = true;
 };
 
 struct DevPlan {
@@ -62,11 +64,14 @@ struct DevPlan {
     FieldTile* d_field = nullptr;
     int n_move = 0, n_field = 0;
     int max_tile_beads = 0, max_length = 0, n_types_uniform = 0;
+    bool linear = false;
     scmf_tune tune{};
     cudaGraphExec_t graph = nullptr;
     cudaGraph_t graph_src = nullptr;
     void release();
     scmf_status upload(const Plan& p, const scmf_tune& t);
+    LaunchShape move_shape() const;
+    LaunchShape field_shape() const;
     // one fused sweep (move+grid, field) enqueued on `st`
     scmf_status enqueue_sweep(cudaStream_t st) const;
     scmf_status run_sweeps(cudaStream_t st, int n);

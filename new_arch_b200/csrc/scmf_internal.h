@@ -104,6 +104,7 @@ struct LaunchShape {
     int threads;
     int smem;      // unused by the launchers (they size shared memory themselves)
     int n_types;   // field kernel: monomer types shared by all systems, 0 = mixed
+    int linear;    // sweep kernel: every architecture is a linear chain
 };
 
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);

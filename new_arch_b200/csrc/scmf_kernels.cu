@@ -79,38 +79,39 @@ __device__ __forceinline__ int cell_of(const MoveConsts& c, float x, float y, fl
     return ix + c.nx * (iy + c.ny * iz);
 }
 
-// One smart-MC trial of bead b of the chain whose beads start at smem offset
-// `base`.  Same expression order as the oracle's move_bead().
-__device__ __forceinline__ int move_bead(const MoveConsts& c, const BeadInfo& bi, float* sx, float* sy,
-                                         float* sz, int base, int b, uint32_t gc, uint32_t step,
-                                         uint32_t k0, uint32_t k1, const float* __restrict__ w_t) {
+// One smart-MC trial (device_function.cu:637-717, 562-588, 444-454) of a bead
+// at (x,y,z) with deg bonded neighbours q[0..deg) in ascending bead order.
+// Same expression order as the oracle's move_bead().  On return (px,py,pz) is
+// the bead's final position; eb gains k |r - q_d|^2 of the final position for
+// every neighbour d flagged in lower_mask (neighbours of a lower colour, which
+// have already made their final move this sweep).
+template <int MAXDEG>
+__device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, float z, const float* qx,
+                                      const float* qy, const float* qz, int deg, unsigned lower_mask, uint4 w,
+                                      const float* __restrict__ w_t, float& px, float& py, float& pz, float& eb) {
     const float k = c.k, k2 = c.k2, A = c.A, R = c.R;
-    const int deg = bi.deg;
-    const float x = sx[base + b], y = sy[base + b], z = sz[base + b];
-    float qx[kMaxDeg], qy[kMaxDeg], qz[kMaxDeg];
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
 #pragma unroll
-    for (int d = 0; d < kMaxDeg; ++d) {
+    for (int d = 0; d < MAXDEG; ++d) {
         if (d < deg) {
-            const int j = base + bi.nbr[d];
-            qx[d] = sx[j];
-            qy[d] = sy[j];
-            qz[d] = sz[j];
             fx = fx + (qx[d] - x) * k2;
             fy = fy + (qy[d] - y) * k2;
             fz = fz + (qz[d] - z) * k2;
         }
     }
     float n0, n1, n2;
-    normals3(philox4x32_10(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1), n0, n1, n2);
+    normals3(w, n0, n1, n2);
     const float dx = A * fx + R * n0;
     const float dy = A * fy + R * n1;
     const float dz = A * fz + R * n2;
-    const float px = x + dx, py = y + dy, pz = z + dz;
+    px = x + dx;
+    py = y + dy;
+    pz = z + dz;
     float nfx = 0.0f, nfy = 0.0f, nfz = 0.0f;
     float deb = 0.0f;
+    float o2s[MAXDEG], e2s[MAXDEG];
 #pragma unroll
-    for (int d = 0; d < kMaxDeg; ++d) {
+    for (int d = 0; d < MAXDEG; ++d) {
         if (d < deg) {
             nfx = nfx + (qx[d] - px) * k2;
             nfy = nfy + (qy[d] - py) * k2;
@@ -119,6 +120,8 @@ __device__ __forceinline__ int move_bead(const MoveConsts& c, const BeadInfo& bi
             const float ex = ox + dx, ey = oy + dy, ez = oz + dz;
             const float o2 = ox * ox + oy * oy + oz * oz;
             const float e2 = ex * ex + ey * ey + ez * ez;
+            o2s[d] = o2;
+            e2s[d] = e2;
             deb = deb + k * (e2 - o2);
         }
     }
@@ -128,19 +131,23 @@ __device__ __forceinline__ int move_bead(const MoveConsts& c, const BeadInfo& bi
     const float w_new = __ldg(w_t + cell_of(c, px, py, pz));
     float dE = (w_new - w_old) + deb;
     dE = dE + smc;
+    // log(u) >= -24 ln2 > -17 for every u the generator yields: dE >= 17 rejects
     bool acc;
-    if (dE < 0.0f) {
+    if (dE < 0.0f)
         acc = true;
-    } else {
-        const uint4 u = philox4x32_10(make_uint4(gc, (uint32_t)b, step, 1u), k0, k1);
-        acc = log_f(u01(u.x)) < -dE;
+    else if (dE < 17.0f)
+        acc = log_f(u01(accept_word(w))) < -dE;
+    else
+        acc = false;
+    if (!acc) {
+        px = x;
+        py = y;
+        pz = z;
     }
-    if (acc) {
-        sx[base + b] = px;
-        sy[base + b] = py;
-        sz[base + b] = pz;
-    }
-    return acc ? 1 : 0;
+#pragma unroll
+    for (int d = 0; d < MAXDEG; ++d)
+        if (d < deg && (lower_mask >> d) & 1u) eb += k * (acc ? e2s[d] : o2s[d]);
+    return acc;
 }
 
 template <typename T>
@@ -159,9 +166,14 @@ size_t sweep_smem_bytes(int max_tile_beads, int max_length) {
     return (b + 15) & ~(size_t)15;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(512) k_sweep(const MoveTile* __restrict__ tiles, int n_tiles,
-                                                int max_tile_beads, int max_length) {
+// One MC sweep over tiles of whole chains staged in shared memory.
+//   MODE kMoveOnly / kMoveGrid / kGridOnly: moves, moves + counts of the final
+//   positions into counts[cur^1], counts of the current positions into counts[cur].
+//   LINEAR: every architecture of the launch is a linear chain (bonds i-i+1,
+//   even beads colour 0, odd beads colour 1); neighbours are computed, not looked up.
+template <int MODE, bool LINEAR>
+__global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ tiles, int n_tiles,
+                                                   int max_tile_beads, int max_length) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sx = reinterpret_cast<float*>(smem_raw);
     float* sy = sx + max_tile_beads;
@@ -170,7 +182,8 @@ __global__ void __launch_bounds__(512) k_sweep(const MoveTile* __restrict__ tile
     BeadInfo* sinfo = reinterpret_cast<BeadInfo*>(smem_raw + off);
     off = (off + (size_t)max_length * sizeof(BeadInfo) + 15) & ~(size_t)15;
     uint16_t* scol = reinterpret_cast<uint16_t*>(smem_raw + off);
-    __shared__ double s_eb[32];
+    uint8_t* stype = reinterpret_cast<uint8_t*>(sinfo);  // LINEAR: types only
+    __shared__ float s_eb[32];
     __shared__ unsigned s_acc[32];
 
     const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -190,8 +203,12 @@ __global__ void __launch_bounds__(512) k_sweep(const MoveTile* __restrict__ tile
         c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
         const uint32_t len_magic = Ap->len_magic;
         for (int i = tid; i < L; i += T) {
-            sinfo[i] = Ap->beads[i];
-            scol[i] = Ap->color_beads[i];
+            if (LINEAR) {
+                stype[i] = Ap->beads[i].type;
+            } else {
+                sinfo[i] = Ap->beads[i];
+                scol[i] = Ap->color_beads[i];
+            }
         }
         float* gx = S->x + t.bead0;
         float* gy = S->y + t.bead0;
@@ -220,35 +237,66 @@ __global__ void __launch_bounds__(512) k_sweep(const MoveTile* __restrict__ tile
             const uint32_t step = S->step + 1u;
             const uint32_t k0 = S->seed_lo, k1 = S->seed_hi;
             const uint32_t* __restrict__ cid = S->chain_id + t.chain0;
+            const float* __restrict__ omega = S->omega;
+            const int64_t NC = S->n_cells;
             unsigned nacc = 0;
+            float eb = 0.0f;
             for (int col = 0; col < Ap->n_colors; ++col) {
-                const int c0 = Ap->color_off[col];
-                const int ncol = Ap->color_off[col + 1] - c0;
+                const int ncol = Ap->color_off[col + 1] - Ap->color_off[col];
                 const uint32_t mg = Ap->color_magic[col];
                 const int items = t.n_chains * ncol;
                 for (int j = tid; j < items; j += T) {
                     const int cl = (int)div_magic((uint32_t)j, mg, ncol);
-                    const int b = scol[c0 + (j - cl * ncol)];
-                    const BeadInfo bi = sinfo[b];
-                    const float* w_t = S->omega + (int64_t)bi.type * S->n_cells;
-                    nacc += move_bead(c, bi, sx, sy, sz, cl * L, b, __ldg(cid + cl), step, k0, k1, w_t);
+                    const int base = cl * L;
+                    float qx[LINEAR ? 2 : kMaxDeg], qy[LINEAR ? 2 : kMaxDeg], qz[LINEAR ? 2 : kMaxDeg];
+                    int b, deg, type;
+                    unsigned lower = 0;
+                    if (LINEAR) {
+                        b = 2 * (j - cl * ncol) + col;
+                        type = stype[b];
+                        deg = 0;
+                        if (b > 0) {
+                            qx[0] = sx[base + b - 1];
+                            qy[0] = sy[base + b - 1];
+                            qz[0] = sz[base + b - 1];
+                            deg = 1;
+                        }
+                        if (b + 1 < L) {
+                            qx[deg] = sx[base + b + 1];
+                            qy[deg] = sy[base + b + 1];
+                            qz[deg] = sz[base + b + 1];
+                            ++deg;
+                        }
+                        lower = col == 1 ? 3u : 0u;
+                    } else {
+                        b = scol[Ap->color_off[col] + (j - cl * ncol)];
+                        const BeadInfo bi = sinfo[b];
+                        type = bi.type;
+                        deg = bi.deg;
+#pragma unroll
+                        for (int d = 0; d < kMaxDeg; ++d) {
+                            if (d < deg) {
+                                const int q = base + bi.nbr[d];
+                                qx[d] = sx[q];
+                                qy[d] = sy[q];
+                                qz[d] = sz[q];
+                                if (sinfo[bi.nbr[d]].color < col) lower |= 1u << d;
+                            }
+                        }
+                    }
+                    const uint4 w = philox4x32_10(make_uint4(__ldg(cid + cl), (uint32_t)b, step, 0u), k0, k1);
+                    float px, py, pz;
+                    const bool acc = trial<LINEAR ? 2 : kMaxDeg>(c, sx[base + b], sy[base + b], sz[base + b], qx, qy,
+                                                                 qz, deg, lower, w, omega + (int64_t)type * NC, px,
+                                                                 py, pz, eb);
+                    if (acc) {
+                        sx[base + b] = px;
+                        sy[base + b] = py;
+                        sz[base + b] = pz;
+                    }
+                    nacc += acc ? 1u : 0u;
                 }
                 __syncthreads();
-            }
-            // bond energy of the final positions, each bond once (j > i)
-            double eb = 0.0;
-            for (int i = tid; i < nb; i += T) {
-                const int cl = (int)div_magic((uint32_t)i, len_magic, L);
-                const int b = i - cl * L;
-                const BeadInfo bi = sinfo[b];
-                for (int d = 0; d < bi.deg; ++d) {
-                    const int j = bi.nbr[d];
-                    if (j <= b) continue;
-                    const int jj = cl * L + j;
-                    const float ex = sx[i] - sx[jj], ey = sy[i] - sy[jj], ez = sz[i] - sz[jj];
-                    const float r2 = ex * ex + ey * ey + ez * ez;
-                    eb += (double)c.k * (double)r2;
-                }
             }
             eb = warp_sum(eb);
             nacc = warp_sum(nacc);
@@ -261,7 +309,7 @@ __global__ void __launch_bounds__(512) k_sweep(const MoveTile* __restrict__ tile
                 double e = 0.0;
                 unsigned long long a = 0;
                 for (int w = 0; w < (T + 31) / 32; ++w) {
-                    e += s_eb[w];
+                    e += (double)s_eb[w];
                     a += s_acc[w];
                 }
                 const int slot = ti % kSlots;
@@ -278,7 +326,8 @@ __global__ void __launch_bounds__(512) k_sweep(const MoveTile* __restrict__ tile
             for (int i = tid; i < nb; i += T) {
                 const int cl = (int)div_magic((uint32_t)i, len_magic, L);
                 const int b = i - cl * L;
-                const int64_t idx = (int64_t)sinfo[b].type * NC + cell_of(c, sx[i], sy[i], sz[i]);
+                const int type = LINEAR ? stype[b] : sinfo[b].type;
+                const int64_t idx = (int64_t)type * NC + cell_of(c, sx[i], sy[i], sz[i]);
                 if (c16)
                     atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16));
                 else
@@ -527,13 +576,21 @@ int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_c
 
 // Opt the sweep kernels in to the largest dynamic shared memory once, outside
 // any stream capture (called when a system is created).
+template <int MODE, bool LINEAR>
+static cudaError_t allow_smem(int bytes) {
+    return cudaFuncSetAttribute(k_sweep<MODE, LINEAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 int configure_kernels() {
     static int done = 0;
     if (done) return 0;
     const int bytes = (int)sweep_smem_bytes(kMaxTileBeads, kMaxLength);
-    cudaError_t e = cudaFuncSetAttribute(k_sweep<kMoveOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_sweep<kMoveGrid>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_sweep<kGridOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = allow_smem<kMoveOnly, false>(bytes);
+    if (e == cudaSuccess) e = allow_smem<kMoveGrid, false>(bytes);
+    if (e == cudaSuccess) e = allow_smem<kGridOnly, false>(bytes);
+    if (e == cudaSuccess) e = allow_smem<kMoveOnly, true>(bytes);
+    if (e == cudaSuccess) e = allow_smem<kMoveGrid, true>(bytes);
+    if (e == cudaSuccess) e = allow_smem<kGridOnly, true>(bytes);
     if (e == cudaSuccess) done = 1;
     return (int)e;
 }
@@ -541,9 +598,12 @@ int configure_kernels() {
 template <int MODE>
 static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, LaunchShape sh, cudaStream_t st) {
     const size_t smem = sweep_smem_bytes(mtb, ml);
-    if (mtb > kMaxTileBeads || ml > kMaxLength) return (int)cudaErrorInvalidValue;
+    if (mtb > kMaxTileBeads || ml > kMaxLength || sh.threads > 256) return (int)cudaErrorInvalidValue;
     const int blocks = sh.blocks > 0 ? sh.blocks : n_tiles;
-    k_sweep<MODE><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml);
+    if (sh.linear)
+        k_sweep<MODE, true><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml);
+    else
+        k_sweep<MODE, false><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml);
     return (int)cudaGetLastError();
 }
 

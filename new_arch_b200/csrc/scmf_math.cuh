@@ -19,15 +19,14 @@ namespace scmf {
 
 // Philox4x32-10: Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
 // easy as 1, 2, 3", SC'11.  Round multipliers 0xD2511F53 / 0xCD9E8D57, key
-// increments 0x9E3779B9 / 0xBB67AE85.
+// increments 0x9E3779B9 / 0xBB67AE85.  Each 32x32->64 product is one wide
+// multiply.
 __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        const uint32_t lo0 = 0xD2511F53u * c.x;
-        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
-        const uint32_t lo1 = 0xCD9E8D57u * c.z;
-        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
-        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+        c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1, (uint32_t)p0);
         k0 += 0x9E3779B9u;
         k1 += 0xBB67AE85u;
     }
@@ -40,25 +39,27 @@ __device__ __forceinline__ float u01(uint32_t w) {
 }
 
 // log(x) for normal x > 0.  x = 2^e m with m in [sqrt(1/2), sqrt(2));
-// log m = 2 atanh(s), s = (m - 1)/(m + 1), series to s^11; e ln2 with a 12-bit
-// head of ln2 so that e * head is exact.
+// log m = log1p(t) = t + t^2 Q(t), t = m - 1 (exact), Q of degree 8 fitted by
+// weighted least squares on Chebyshev nodes (gen_log_poly.py); e ln2 with a
+// 12-bit head of ln2 so that e * head is exact.  No division, no branch.
 __device__ __forceinline__ float log_f(float x) {
     const uint32_t ix = __float_as_uint(x);
     int e = (int)(ix >> 23) - 127;
     uint32_t mb = (ix & 0x007FFFFFu) | 0x3F800000u;
-    if (mb > 0x3FB504F3u) {
-        mb -= 0x00800000u;
-        e += 1;
-    }
-    const float m = __uint_as_float(mb);
-    const float s = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
-    const float s2 = __fmul_rn(s, s);
-    float p = 0x1.745d18p-3f;
-    p = __fmaf_rn(p, s2, 0x1.c71c72p-3f);
-    p = __fmaf_rn(p, s2, 0x1.24924ap-2f);
-    p = __fmaf_rn(p, s2, 0x1.99999ap-2f);
-    p = __fmaf_rn(p, s2, 0x1.555556p-1f);
-    const float lm = __fmaf_rn(__fmul_rn(s, s2), p, __fmul_rn(2.0f, s));
+    const bool hi = mb > 0x3FB504F3u;
+    mb = hi ? mb - 0x00800000u : mb;
+    e = hi ? e + 1 : e;
+    const float t = __fsub_rn(__uint_as_float(mb), 1.0f);
+    float q = -0x1.321a4cp-4f;
+    q = __fmaf_rn(q, t, 0x1.068b2ap-3f);
+    q = __fmaf_rn(q, t, -0x1.0f9b0cp-3f);
+    q = __fmaf_rn(q, t, 0x1.22bf86p-3f);
+    q = __fmaf_rn(q, t, -0x1.5424e0p-3f);
+    q = __fmaf_rn(q, t, 0x1.999fc2p-3f);
+    q = __fmaf_rn(q, t, -0x1.000422p-2f);
+    q = __fmaf_rn(q, t, 0x1.555558p-2f);
+    q = __fmaf_rn(q, t, -0x1.fffff8p-2f);
+    const float lm = __fmaf_rn(__fmul_rn(t, t), q, t);
     const float fe = __int2float_rn(e);
     return __fmaf_rn(fe, 0x1.62ep-1f, __fmaf_rn(fe, 0x1.0bfbe8p-15f, lm));
 }
@@ -85,19 +86,16 @@ __device__ __forceinline__ void sincos_turn(uint32_t w, float& s, float& c) {
     cp = __fmaf_rn(cp, g2, 0x1.03c1f0p-2f);
     cp = __fmaf_rn(cp, g2, -0x1.3bd3ccp+0f);
     const float ca = __fmaf_rn(cp, g2, 1.0f);
-    if (q == 0) {
-        s = sa; c = ca;
-    } else if (q == 1) {
-        s = ca; c = -sa;
-    } else if (q == 2) {
-        s = -sa; c = -ca;
-    } else {
-        s = -ca; c = sa;
-    }
+    const bool odd = q & 1, neg_s = q & 2, neg_c = (q == 1) || (q == 2);
+    const float s0 = odd ? ca : sa;
+    const float c0 = odd ? sa : ca;
+    s = neg_s ? -s0 : s0;
+    c = neg_c ? -c0 : c0;
 }
 
 // Three standard normals from one Philox block (Box-Muller on (w.x, w.y) and
-// on (w.z, w.w), the last sine unused).
+// on (w.z, w.w), the last sine unused).  Only bits 8..31 of each word are
+// read; the low bytes feed accept_word().
 __device__ __forceinline__ void normals3(uint4 w, float& n0, float& n1, float& n2) {
     float s, c;
     const float r0 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.x))));
@@ -107,6 +105,12 @@ __device__ __forceinline__ void normals3(uint4 w, float& n0, float& n1, float& n
     const float r1 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.z))));
     sincos_turn(w.w, s, c);
     n2 = __fmul_rn(r1, c);
+}
+
+// The Metropolis uniform of a move: the low bytes of w.y, w.z, w.w of the
+// block that gave its normals (bits the normals never read).
+__device__ __forceinline__ uint32_t accept_word(uint4 w) {
+    return ((w.y & 0xFFu) << 24) | ((w.z & 0xFFu) << 16) | ((w.w & 0xFFu) << 8);
 }
 
 // floor(x * inv_d) mod n, in [0, n).  FP32 restatement of the periodic fold in

@@ -112,6 +112,14 @@ class System:
     def step_async(self, n_sweeps: int = 1) -> None:
         check(lib().scmf_step_async(self._h, int(n_sweeps)))
 
+    def step_profiled(self, n_sweeps: int = 1):
+        """Runs n sweeps launch by launch with CUDA events; returns the summed
+        device milliseconds of the move+grid kernel, of the field kernel, and
+        the device time from the first launch to the end of the last."""
+        a, b, t = C.c_float(), C.c_float(), C.c_float()
+        check(lib().scmf_step_profiled(self._h, int(n_sweeps), C.byref(a), C.byref(b), C.byref(t)))
+        return a.value, b.value, t.value
+
     def synchronize(self) -> None:
         check(lib().scmf_synchronize(self._h))
 
@@ -155,6 +163,9 @@ class Batch:
 
     def step(self, n_sweeps: int = 1) -> None:
         check(lib().scmf_batch_step(self._h, int(n_sweeps)))
+
+    def step_async(self, n_sweeps: int = 1) -> None:
+        check(lib().scmf_batch_step_async(self._h, int(n_sweeps)))
 
     def autotune(self, sweeps_per_trial: int = 2) -> dict:
         t = _lib.Tune()

@@ -7,13 +7,15 @@
  * Build with -ffp-contract=off so that no multiply-add is contracted: every
  * fused multiply-add below is an explicit fmaf() call, and the CUDA side uses
  * the same explicit fused operations with --fmad=false.  Division and sqrtf
- * are IEEE correctly rounded on both sides.
+ * are IEEE correctly rounded on both sides.  Chain and bead indices key the
+ * generator, so the storage order of chains does not matter either.
  *
  * Algorithm (one sweep at step s):
  *   for every chain, for colour c = 0 .. n_colours-1, for every bead b of
  *   colour c: a smart-MC (force-biased, Rossky-Doll-Friedman) trial against the
- *   frozen omega field, with the Philox4x32-10 counter (chain, b, s, 0) for the
- *   Gaussian displacement and (chain, b, s, 1) for the acceptance uniform.
+ *   frozen omega field.  One Philox4x32-10 block with counter (chain, b, s, 0)
+ *   gives the three Gaussian displacement components and, from the bytes the
+ *   normals do not read, the Metropolis uniform.
  *   Bonded beads never share a colour, so the result does not depend on the
  *   order in which beads of one colour are visited, nor on chain order.
  * The reference instead draws `length` random beads with replacement per chain
@@ -62,22 +64,25 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
 float orc_u01(uint32_t w) { return (float)((w >> 8) | 1u) * 0x1p-24f; }
 
 /* Natural log for normal positive floats: x = 2^e m, m in [sqrt(1/2), sqrt(2)),
- * log m = 2 atanh(s), s = (m-1)/(m+1), odd series to s^11; e ln2 added with a
- * two-part ln2 (12-bit head so that e*head is exact). */
+ * log m = log1p(t) = t + t^2 Q(t), t = m - 1 (exact), Q of degree 8 fitted by
+ * weighted least squares on Chebyshev nodes (new_arch_b200/csrc/gen_log_poly.py);
+ * e ln2 added with a two-part ln2 (12-bit head so that e*head is exact). */
 float orc_logf(float x) {
     uint32_t ix = f2u(x);
     int e = (int)(ix >> 23) - 127;
     uint32_t mb = (ix & 0x007FFFFFu) | 0x3F800000u;
     if (mb > 0x3FB504F3u) { mb -= 0x00800000u; e += 1; }
-    float m = u2f(mb);
-    float s = (m - 1.0f) / (m + 1.0f);
-    float s2 = s * s;
-    float p = 0x1.745d18p-3f;               /* 2/11 */
-    p = fmaf(p, s2, 0x1.c71c72p-3f);        /* 2/9 */
-    p = fmaf(p, s2, 0x1.24924ap-2f);        /* 2/7 */
-    p = fmaf(p, s2, 0x1.99999ap-2f);        /* 2/5 */
-    p = fmaf(p, s2, 0x1.555556p-1f);        /* 2/3 */
-    float lm = fmaf(s * s2, p, 2.0f * s);
+    float t = u2f(mb) - 1.0f;
+    float q = -0x1.321a4cp-4f;
+    q = fmaf(q, t, 0x1.068b2ap-3f);
+    q = fmaf(q, t, -0x1.0f9b0cp-3f);
+    q = fmaf(q, t, 0x1.22bf86p-3f);
+    q = fmaf(q, t, -0x1.5424e0p-3f);
+    q = fmaf(q, t, 0x1.999fc2p-3f);
+    q = fmaf(q, t, -0x1.000422p-2f);
+    q = fmaf(q, t, 0x1.555558p-2f);
+    q = fmaf(q, t, -0x1.fffff8p-2f);
+    float lm = fmaf(t * t, q, t);
     float fe = (float)e;
     return fmaf(fe, 0x1.62ep-1f, fmaf(fe, 0x1.0bfbe8p-15f, lm));
 }
@@ -114,7 +119,8 @@ void orc_sincos_turn(uint32_t w, float* s, float* c) {
 
 /* Three standard normals from one Philox block: Box-Muller on (w0,w1) gives
  * n0 = r cos, n1 = r sin; on (w2,w3) gives n2 = r cos (the fourth is unused,
- * as curand_normal4's w is unused in device_function.cu:683-688). */
+ * as curand_normal4's w is unused in device_function.cu:683-688).  Only bits
+ * 8..31 of each word are read; the low bytes feed orc_accept_word(). */
 void orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2) {
     float s, c;
     float r0 = sqrtf(-2.0f * orc_logf(orc_u01(w[0])));
@@ -124,6 +130,12 @@ void orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2) {
     float r1 = sqrtf(-2.0f * orc_logf(orc_u01(w[2])));
     orc_sincos_turn(w[3], &s, &c);
     *n2 = r1 * c;
+}
+
+/* The Metropolis uniform of a move comes from the same Philox block: the low
+ * bytes of w1, w2, w3, which the normals never read. */
+uint32_t orc_accept_word(const uint32_t w[4]) {
+    return ((w[1] & 0xFFu) << 24) | ((w[2] & 0xFFu) << 16) | ((w[3] & 0xFFu) << 8);
 }
 
 /* Periodic fold of one coordinate to a cell index in [0, n): floor(x/dx) mod n.
@@ -360,9 +372,12 @@ static inline int64_t cell_of(const orc_system* s, float x, float y, float z) {
     return (int64_t)ix + (int64_t)s->nx * ((int64_t)iy + (int64_t)s->ny * iz);
 }
 
-/* One smart-MC trial of bead b (device_function.cu:637-717, 562-588, 444-454). */
+/* One smart-MC trial of bead b (device_function.cu:637-717, 562-588, 444-454).
+ * Returns 1 if accepted; adds to *eb the bond energy k |r_b - r_j|^2 of the
+ * final position of b for every neighbour j of lower colour (final by then),
+ * so every bond is counted once per sweep. */
 static inline int move_bead(const orc_system* s, const orc_arch* a, uint32_t gc, int b,
-                            float* X, float* Y, float* Z, const uint32_t key[2], uint32_t step) {
+                            float* X, float* Y, float* Z, const uint32_t key[2], uint32_t step, float* eb) {
     const int* nb = a->nbr + b * ORC_MAX_DEG;
     const int deg = a->deg[b];
     const float k = s->k, k2 = s->k2, A = s->A, R = s->R;
@@ -384,6 +399,7 @@ static inline int move_bead(const orc_system* s, const orc_arch* a, uint32_t gc,
     float px = x + dx, py = y + dy, pz = z + dz;
     float nfx = 0.0f, nfy = 0.0f, nfz = 0.0f;
     float deb = 0.0f;
+    float o2s[ORC_MAX_DEG], e2s[ORC_MAX_DEG];
     for (int d = 0; d < deg; ++d) {
         int j = nb[d];
         float qx = X[j], qy = Y[j], qz = Z[j];
@@ -394,6 +410,8 @@ static inline int move_bead(const orc_system* s, const orc_arch* a, uint32_t gc,
         float ex = ox + dx, ey = oy + dy, ez = oz + dz;
         float o2 = ox * ox + oy * oy + oz * oz;
         float e2 = ex * ex + ey * ey + ez * ez;
+        o2s[d] = o2;
+        e2s[d] = e2;
         deb = deb + k * (e2 - o2);
     }
     float smc = 0.5f * ((nfx + fx) * dx + (nfy + fy) * dy + (nfz + fz) * dz)
@@ -404,29 +422,17 @@ static inline int move_bead(const orc_system* s, const orc_arch* a, uint32_t gc,
     float w_new = W[cell_of(s, px, py, pz)];
     float dE = (w_new - w_old) + deb;
     dE = dE + smc;
+    /* Metropolis: accept if dE < 0, else if log(u) < -dE.  log(u) >= -24 ln2
+     * > -17 for every u the generator yields, so dE >= 17 always rejects. */
     int acc;
-    if (dE < 0.0f) {
-        acc = 1;
-    } else {
-        uint32_t c2[4] = {gc, (uint32_t)b, step, 1u};
-        orc_philox4x32_10(c2, key, w);
-        acc = orc_logf(orc_u01(w[0])) < -dE;
-    }
+    if (dE < 0.0f) acc = 1;
+    else if (dE < 17.0f) acc = orc_logf(orc_u01(orc_accept_word(w))) < -dE;
+    else acc = 0;
     if (acc) { X[b] = px; Y[b] = py; Z[b] = pz; }
+    const int cb = a->color[b];
+    for (int d = 0; d < deg; ++d)
+        if (a->color[nb[d]] < cb) *eb += k * (acc ? e2s[d] : o2s[d]);
     return acc;
-}
-
-static double chain_bond_energy(const orc_system* s, const orc_arch* a, const float* X, const float* Y, const float* Z) {
-    double e = 0.0;
-    for (int i = 0; i < a->length; ++i)
-        for (int d = 0; d < a->deg[i]; ++d) {
-            int j = a->nbr[i * ORC_MAX_DEG + d];
-            if (j <= i) continue;
-            float ex = X[i] - X[j], ey = Y[i] - Y[j], ez = Z[i] - Z[j];
-            float r2 = ex * ex + ey * ey + ez * ez;
-            e += (double)s->k * (double)r2;
-        }
-    return e;
 }
 
 static void sweep_moves(orc_system* s, uint32_t step) {
@@ -439,11 +445,12 @@ static void sweep_moves(orc_system* s, uint32_t step) {
             float* X = s->x + b0; float* Y = s->y + b0; float* Z = s->z + b0;
             uint32_t gc = (uint32_t)(ar->chain_base + c);
             uint32_t nacc = 0;
+            float eb = 0.0f;
             for (int col = 0; col < ar->n_colors; ++col)
                 for (int b = 0; b < ar->length; ++b)
-                    if (ar->color[b] == col) nacc += (uint32_t)move_bead(s, ar, gc, b, X, Y, Z, key, step);
+                    if (ar->color[b] == col) nacc += (uint32_t)move_bead(s, ar, gc, b, X, Y, Z, key, step, &eb);
             s->chain_acc[ar->chain_base + c] = nacc;
-            s->chain_ebond[ar->chain_base + c] = chain_bond_energy(s, ar, X, Y, Z);
+            s->chain_ebond[ar->chain_base + c] = (double)eb;
         }
     }
     uint64_t acc = 0; double eb = 0.0;
