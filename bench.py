@@ -204,19 +204,17 @@ def run_ours(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
+    from new_arch_b200.replicas import gather_ints, reduce_max, replica_seed, whole_job_rate
+
     def barrier():
         if dist is not None:
             dist.barrier()
 
     def allmax(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(v, dist, "cuda")
 
-    # ---- plain large system: the headline step
-    spec = large_system(seed=7 + rank)
+    # ---- plain large system: the headline step (one replica per rank)
+    spec = large_system(seed=replica_seed(7, rank))
     s = nb.System(spec)
     s.init_coords()
     s.step(args.warmup)
@@ -231,7 +229,8 @@ def run_ours(args):
     ms_total = allmax(ms_total)
     st = s.stats()
     accept_ratio = st["last_accepts"] / spec.n_beads
-    value = world * spec.n_beads * args.steps / (ms_total / 1e3)
+    beads_all = gather_ints(spec.n_beads, dist, "cuda")
+    value = whole_job_rate(beads_all, args.steps, ms_total / 1e3)
     peak, peak_kind = measured_peaks()
     alg_bytes = 24 * spec.n_beads + 4 * spec.n_types * spec.n_cells          # move+grid kernel per launch
     achieved = alg_bytes / (ms_move / args.steps / 1e3) / 1e9
@@ -252,7 +251,7 @@ def run_ours(args):
         s.stats()
     cnt = s.counts()
     e2e_s = allmax(time.perf_counter() - t0)
-    e2e = {"value": world * spec.n_beads * args.steps / e2e_s, "unit": UNIT,
+    e2e = {"value": whole_job_rate(beads_all, args.steps, e2e_s), "unit": UNIT,
            "h2d_bytes_per_step": xyz.nbytes / args.steps,
            "d2h_bytes_per_step": (64 * args.steps + cnt.nbytes) / args.steps,
            "how": "wall clock around scmf_set_coords(pinned host xyz) + K x (scmf_step(1) + scmf_get_stats) + scmf_get_counts"}

@@ -25,7 +25,7 @@ CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-std=c++17",
-                     "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC]
+                     "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC] + os.environ.get("SCMF_NVCC_EXTRA", "").split()
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-result", "-ffp-contract=off", "-pthread",
              "-I" + INC, "-I" + CSRC, "-I" + os.path.join(CUDA, "include")]
 

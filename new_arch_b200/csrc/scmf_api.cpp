@@ -282,7 +282,8 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
         return bail(rc);
     // architecture tables
     size_t blob = 0;
-    for (const auto& a : s->archs) blob += round_up((size_t)a.length * (sizeof(BeadInfo) + sizeof(uint16_t)), 256);
+    auto arch_bytes = [](int L) { return round_up((size_t)L * (sizeof(BeadInfo) + sizeof(uint16_t) + 1) + 16, 256); };
+    for (const auto& a : s->archs) blob += arch_bytes(a.length);
     if ((rc = dalloc(&s->d_arch_blob, blob, &tot))) return bail(rc);
     s->device_bytes = tot;
     std::vector<char> hblob(blob, 0);
@@ -294,11 +295,17 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
         const size_t off2 = off + (size_t)a.length * sizeof(BeadInfo);
         std::memcpy(hblob.data() + off2, a.color_beads.data(), a.length * sizeof(uint16_t));
         d.color_beads = (const uint16_t*)((char*)s->d_arch_blob + off2);
-        off += round_up((size_t)a.length * (sizeof(BeadInfo) + sizeof(uint16_t)), 256);
+        const size_t off3 = off2 + (size_t)a.length * sizeof(uint16_t);
+        for (int i = 0; i < a.length; ++i) hblob[off3 + i] = (char)a.beads[i].type;
+        d.types = (const uint8_t*)((char*)s->d_arch_blob + off3);
+        off += arch_bytes(a.length);
         d.length = a.length;
         d.n_colors = a.n_colors;
         for (int c = 0; c <= a.n_colors; ++c) d.color_off[c] = a.color_off[c];
-        for (int c = 0; c < a.n_colors; ++c) d.color_magic[c] = magic_for((uint32_t)(a.color_off[c + 1] - a.color_off[c]));
+        for (int c = 0; c < a.n_colors; ++c) {
+            const uint32_t nc = (uint32_t)(a.color_off[c + 1] - a.color_off[c]);
+            d.color_magic[c] = magic_for(nc);
+        }
         d.len_magic = magic_for((uint32_t)a.length);
         d.n_chains = a.n_chains;
         d.chain_base = a.chain_base;
@@ -507,10 +514,15 @@ scmf_status scmf_set_omega(scmf_system* s, const float* in, size_t n) {
     return SCMF_OK;
 }
 
-scmf_status scmf_get_stats(const scmf_system* s, scmf_stats* o) {
+scmf_status scmf_get_stats(const scmf_system* cs, scmf_stats* o) {
+    scmf_system* s = const_cast<scmf_system*>(cs);
     if (!s || !o) return fail(SCMF_E_INVALID, "NULL argument");
     SysDev d;
     RET(fetch_sysdev(s, &d));
+    if (d.e_bond_step != d.step + 1u) {  // bond energy is computed on demand
+        CKL(launch_bond_energy(s->plan.d_move, s->plan.n_move, s->d_sys, s->plan.move_shape(), s->stream));
+        RET(fetch_sysdev(s, &d));
+    }
     std::memset(o, 0, sizeof *o);
     o->step = d.step;
     o->last_accepts = d.last_accepts;

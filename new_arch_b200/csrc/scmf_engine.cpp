@@ -162,7 +162,7 @@ size_t system_device_bytes(const scmf_spec& s) {
     for (const auto& a : s.archs) {
         beads += (int64_t)a.length * a.n_chains;
         chains += a.n_chains;
-        arch_bytes += round_up((size_t)a.length * (sizeof(BeadInfo) + 2), 256);
+        arch_bytes += round_up((size_t)a.length * (sizeof(BeadInfo) + 3) + 16, 256);
     }
     const size_t cells = (size_t)s.nx * s.ny * s.nz * s.n_types;
     size_t b = 3 * round_up((size_t)(beads + 4) * 4, 256) + round_up((size_t)chains * 4, 256);
@@ -187,6 +187,10 @@ void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d) {
     d->k2 = (float)(2.0 * s.p.harmonic_normb);
     d->A = (float)s.p.smc_a;
     d->R = (float)std::sqrt(2.0 * s.p.smc_a);
+    for (int g = 0; g <= kMaxDeg; ++g) {
+        d->cdeg[g] = d->k2 * (float)g;
+        d->ac4deg[g] = (d->A * d->cdeg[g]) * 0.25f;
+    }
     const double inv_n = 1.0 / (double)s.p.reference_nbeads;
     const int n = s.n_types;
     for (int i = 0; i < kMaxTypes * kMaxTypes; ++i) d->cf[i] = 0.0f;
@@ -251,6 +255,7 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t) {
     max_tile_beads = p.max_tile_beads;
     max_length = p.max_length;
     n_types_uniform = p.n_types_uniform;
+    max_chains = p.max_chains;
     linear = p.linear;
     CK(cudaMalloc(&d_move, std::max<size_t>(1, p.move.size()) * sizeof(MoveTile)));
     CK(cudaMalloc(&d_field, std::max<size_t>(1, p.field.size()) * sizeof(FieldTile)));
@@ -265,6 +270,7 @@ LaunchShape DevPlan::move_shape() const {
     sh.threads = tune.threads_move;
     sh.n_types = n_types_uniform;
     sh.linear = linear ? 1 : 0;
+    sh.max_chains = max_chains;
     return sh;
 }
 
@@ -322,6 +328,7 @@ using namespace scmf;
 // Work tiles of this system appended to a plan.
 scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
     const int64_t target_small = std::max<int64_t>(1, n_beads / (2 * 148));
+    const size_t first_tile = p->move.size();
     for (size_t a = 0; a < archs.size(); ++a) {
         const ArchHost& A = archs[a];
         if (A.n_chains == 0) continue;
@@ -338,15 +345,20 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
             mt.chain0 = A.chain_base + c;
             mt.n_chains = std::min(cpt, A.n_chains - c);
             mt.bead0 = A.bead_base + (int64_t)c * A.length;
+            mt.n_tiles_sys = 0;
+            mt.pad = 0;
             p->move.push_back(mt);
             p->max_tile_beads = std::max(p->max_tile_beads, mt.n_chains * A.length);
+            p->max_chains = std::max(p->max_chains, mt.n_chains);
         }
         p->max_length = std::max(p->max_length, A.length);
         p->max_deg = std::max(p->max_deg, A.max_deg);
         p->linear = p->linear && A.linear;
     }
+    for (size_t i = first_tile; i < p->move.size(); ++i) p->move[i].n_tiles_sys = (int32_t)(p->move.size() - first_tile);
     int64_t cpt_cells = t.cells_per_tile;
-    if (cpt_cells <= 0) cpt_cells = std::min<int64_t>(16384, std::max<int64_t>(1024, n_cells / (2 * 148)));
+    if (cpt_cells <= 0) cpt_cells = std::min<int64_t>(8192, std::max<int64_t>(1024, n_cells / (4 * 148)));
+    cpt_cells = (cpt_cells + 3) & ~(int64_t)3;
     const int ntile = (int)((n_cells + cpt_cells - 1) / cpt_cells);
     for (int i = 0; i < ntile; ++i) {
         FieldTile ft;

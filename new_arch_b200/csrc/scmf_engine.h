@@ -56,6 +56,7 @@ struct Plan {
     int max_length = 0;
     int n_types_uniform = 0;
     int max_deg = 0;
+    int max_chains = 0;   // most chains in one move tile
     bool linear = true;
 };
 
@@ -63,7 +64,7 @@ struct DevPlan {
     MoveTile* d_move = nullptr;
     FieldTile* d_field = nullptr;
     int n_move = 0, n_field = 0;
-    int max_tile_beads = 0, max_length = 0, n_types_uniform = 0;
+    int max_tile_beads = 0, max_length = 0, n_types_uniform = 0, max_chains = 0;
     bool linear = false;
     scmf_tune tune{};
     cudaGraphExec_t graph = nullptr;

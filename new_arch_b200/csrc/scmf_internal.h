@@ -39,6 +39,7 @@ struct BeadInfo {
 struct ArchDev {
     const BeadInfo* beads;       // [length]
     const uint16_t* color_beads; // [length], beads grouped by colour
+    const uint8_t* types;        // [length], monomer type per bead
     int32_t length;
     int32_t n_colors;
     int32_t color_off[kMaxColors + 1];
@@ -63,6 +64,8 @@ struct SysDev {
     float inv_dx, inv_dy, inv_dz, scale;
     float lx, ly, lz;
     float k, k2, A, R;
+    float cdeg[kMaxDeg + 1];    // c = 2k deg
+    float ac4deg[kMaxDeg + 1];  // A c / 4
     float cf[kMaxTypes * kMaxTypes];
     int32_t hamiltonian, field_rule, count16, n_arch;
     uint32_t seed_lo, seed_hi;
@@ -77,6 +80,8 @@ struct SysDev {
     // statistics of the last completed sweep
     unsigned long long last_accepts, total_accepts, total_moves;
     double e_bond, e_field;
+    uint32_t e_bond_step;  // step at which e_bond was last computed (+1; 0 = never)
+    uint32_t pad1;
 };
 
 // Work item of the move / grid kernel: a run of whole chains of one architecture.
@@ -86,6 +91,8 @@ struct MoveTile {
     int32_t chain0;       // first storage slot (system-wide chain index)
     int32_t n_chains;
     int64_t bead0;        // first bead (system arrays)
+    int32_t n_tiles_sys;  // move tiles of this system in the launch
+    int32_t pad;
 };
 
 // Work item of the field kernel: a run of cells of one system.
@@ -105,6 +112,7 @@ struct LaunchShape {
     int smem;      // unused by the launchers (they size shared memory themselves)
     int n_types;   // field kernel: monomer types shared by all systems, 0 = mixed
     int linear;    // sweep kernel: every architecture is a linear chain
+    int max_chains;  // sweep kernel: most chains in one tile
 };
 
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);
@@ -113,6 +121,7 @@ int launch_sweep(int mode, const MoveTile* tiles, int n_tiles, int max_tile_bead
 int launch_field(bool fused, int force_update, const FieldTile* tiles, int n_tiles, LaunchShape shape,
                  void* stream);
 int launch_finalize_move(SysDev* sys, void* stream);
+int launch_bond_energy(const MoveTile* tiles, int n_tiles, SysDev* sys, LaunchShape shape, void* stream);
 int launch_aos_to_soa(const float* aos, SysDev* sys, const ArchDev* arch, int n_arch, int64_t n_beads,
                       void* stream);
 int launch_soa_to_aos(float* aos, const SysDev* sys, const ArchDev* arch, int n_arch, int64_t n_beads,

@@ -81,57 +81,41 @@ __device__ __forceinline__ int cell_of(const MoveConsts& c, float x, float y, fl
 
 // One smart-MC trial (device_function.cu:637-717, 562-588, 444-454) of a bead
 // at (x,y,z) with deg bonded neighbours q[0..deg) in ascending bead order.
-// Same expression order as the oracle's move_bead().  On return (px,py,pz) is
-// the bead's final position; eb gains k |r - q_d|^2 of the final position for
-// every neighbour d flagged in lower_mask (neighbours of a lower colour, which
-// have already made their final move this sweep).
+// With f = 2k sum_j (q_j - p) the force and d = A f + R xi the displacement,
+// the reference's bonded energy change plus smart-MC correction equals
+// (A c / 4)(c |d|^2 - 2 f.d), c = 2k deg (the force at p + d is f - c d).
+// Same FP32 expression (explicit fma) as the oracle's move_bead().  Returns
+// whether the move is accepted; (px,py,pz) is the final position and cell the
+// final cell index.
 template <int MAXDEG>
 __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, float z, const float* qx,
-                                      const float* qy, const float* qz, int deg, unsigned lower_mask, uint4 w,
-                                      const float* __restrict__ w_t, float& px, float& py, float& pz, float& eb) {
-    const float k = c.k, k2 = c.k2, A = c.A, R = c.R;
+                                      const float* qy, const float* qz, int deg, float cc, float ac4, uint4 w,
+                                      const float* __restrict__ w_t, float& px, float& py, float& pz, int& cell) {
+    const float k2 = c.k2, A = c.A, R = c.R;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
 #pragma unroll
     for (int d = 0; d < MAXDEG; ++d) {
         if (d < deg) {
-            fx = fx + (qx[d] - x) * k2;
-            fy = fy + (qy[d] - y) * k2;
-            fz = fz + (qz[d] - z) * k2;
+            fx = __fmaf_rn(__fsub_rn(qx[d], x), k2, fx);
+            fy = __fmaf_rn(__fsub_rn(qy[d], y), k2, fy);
+            fz = __fmaf_rn(__fsub_rn(qz[d], z), k2, fz);
         }
     }
     float n0, n1, n2;
     normals3(w, n0, n1, n2);
-    const float dx = A * fx + R * n0;
-    const float dy = A * fy + R * n1;
-    const float dz = A * fz + R * n2;
-    px = x + dx;
-    py = y + dy;
-    pz = z + dz;
-    float nfx = 0.0f, nfy = 0.0f, nfz = 0.0f;
-    float deb = 0.0f;
-    float o2s[MAXDEG], e2s[MAXDEG];
-#pragma unroll
-    for (int d = 0; d < MAXDEG; ++d) {
-        if (d < deg) {
-            nfx = nfx + (qx[d] - px) * k2;
-            nfy = nfy + (qy[d] - py) * k2;
-            nfz = nfz + (qz[d] - pz) * k2;
-            const float ox = x - qx[d], oy = y - qy[d], oz = z - qz[d];
-            const float ex = ox + dx, ey = oy + dy, ez = oz + dz;
-            const float o2 = ox * ox + oy * oy + oz * oz;
-            const float e2 = ex * ex + ey * ey + ez * ez;
-            o2s[d] = o2;
-            e2s[d] = e2;
-            deb = deb + k * (e2 - o2);
-        }
-    }
-    const float smc = 0.5f * ((nfx + fx) * dx + (nfy + fy) * dy + (nfz + fz) * dz) +
-                      0.25f * A * (nfx * nfx + nfy * nfy + nfz * nfz - fx * fx - fy * fy - fz * fz);
-    const float w_old = __ldg(w_t + cell_of(c, x, y, z));
-    const float w_new = __ldg(w_t + cell_of(c, px, py, pz));
-    float dE = (w_new - w_old) + deb;
-    dE = dE + smc;
-    // log(u) >= -24 ln2 > -17 for every u the generator yields: dE >= 17 rejects
+    const float dx = __fmaf_rn(A, fx, __fmul_rn(R, n0));
+    const float dy = __fmaf_rn(A, fy, __fmul_rn(R, n1));
+    const float dz = __fmaf_rn(A, fz, __fmul_rn(R, n2));
+    px = __fadd_rn(x, dx);
+    py = __fadd_rn(y, dy);
+    pz = __fadd_rn(z, dz);
+    const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+    const float fd = __fmaf_rn(fx, dx, __fmaf_rn(fy, dy, __fmul_rn(fz, dz)));
+    const float deb = __fmul_rn(ac4, __fmaf_rn(cc, d2, __fmul_rn(-2.0f, fd)));
+    const int c_old = cell_of(c, x, y, z);
+    const int c_new = cell_of(c, px, py, pz);
+    const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + c_new), __ldg(w_t + c_old)), deb);
+    // log(u) >= -23 ln2 > -17 for every u the generator yields: dE >= 17 rejects
     bool acc;
     if (dE < 0.0f)
         acc = true;
@@ -139,14 +123,7 @@ __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, flo
         acc = log_f(u01(accept_word(w))) < -dE;
     else
         acc = false;
-    if (!acc) {
-        px = x;
-        py = y;
-        pz = z;
-    }
-#pragma unroll
-    for (int d = 0; d < MAXDEG; ++d)
-        if (d < deg && (lower_mask >> d) & 1u) eb += k * (acc ? e2s[d] : o2s[d]);
+    cell = acc ? c_new : c_old;
     return acc;
 }
 
@@ -183,7 +160,6 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
     off = (off + (size_t)max_length * sizeof(BeadInfo) + 15) & ~(size_t)15;
     uint16_t* scol = reinterpret_cast<uint16_t*>(smem_raw + off);
     uint8_t* stype = reinterpret_cast<uint8_t*>(sinfo);  // LINEAR: types only
-    __shared__ float s_eb[32];
     __shared__ unsigned s_acc[32];
 
     const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -239,8 +215,10 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
             const uint32_t* __restrict__ cid = S->chain_id + t.chain0;
             const float* __restrict__ omega = S->omega;
             const int64_t NC = S->n_cells;
+            const float cc2 = S->cdeg[2], ac42 = S->ac4deg[2];
+            uint32_t* cnt = S->counts[S->cur ^ 1u];
+            const bool c16 = S->count16 != 0;
             unsigned nacc = 0;
-            float eb = 0.0f;
             for (int col = 0; col < Ap->n_colors; ++col) {
                 const int ncol = Ap->color_off[col + 1] - Ap->color_off[col];
                 const uint32_t mg = Ap->color_magic[col];
@@ -250,7 +228,6 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
                     const int base = cl * L;
                     float qx[LINEAR ? 2 : kMaxDeg], qy[LINEAR ? 2 : kMaxDeg], qz[LINEAR ? 2 : kMaxDeg];
                     int b, deg, type;
-                    unsigned lower = 0;
                     if (LINEAR) {
                         b = 2 * (j - cl * ncol) + col;
                         type = stype[b];
@@ -267,7 +244,6 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
                             qz[deg] = sz[base + b + 1];
                             ++deg;
                         }
-                        lower = col == 1 ? 3u : 0u;
                     } else {
                         b = scol[Ap->color_off[col] + (j - cl * ncol)];
                         const BeadInfo bi = sinfo[b];
@@ -280,45 +256,43 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
                                 qx[d] = sx[q];
                                 qy[d] = sy[q];
                                 qz[d] = sz[q];
-                                if (sinfo[bi.nbr[d]].color < col) lower |= 1u << d;
                             }
                         }
                     }
                     const uint4 w = philox4x32_10(make_uint4(__ldg(cid + cl), (uint32_t)b, step, 0u), k0, k1);
                     float px, py, pz;
+                    int cell;
                     const bool acc = trial<LINEAR ? 2 : kMaxDeg>(c, sx[base + b], sy[base + b], sz[base + b], qx, qy,
-                                                                 qz, deg, lower, w, omega + (int64_t)type * NC, px,
-                                                                 py, pz, eb);
+                                                                 qz, deg, deg == 2 ? cc2 : S->cdeg[deg],
+                                                                 deg == 2 ? ac42 : S->ac4deg[deg], w,
+                                                                 omega + (int64_t)type * NC, px, py, pz, cell);
                     if (acc) {
                         sx[base + b] = px;
                         sy[base + b] = py;
                         sz[base + b] = pz;
                     }
                     nacc += acc ? 1u : 0u;
+                    if (MODE == kMoveGrid) {
+                        const int64_t idx = (int64_t)type * NC + cell;
+                        if (c16)
+                            atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16));
+                        else
+                            atomicAdd(cnt + idx, 1u);
+                    }
                 }
                 __syncthreads();
             }
-            eb = warp_sum(eb);
             nacc = warp_sum(nacc);
-            if (lane == 0) {
-                s_eb[warp] = eb;
-                s_acc[warp] = nacc;
-            }
+            if (lane == 0) s_acc[warp] = nacc;
             __syncthreads();
             if (tid == 0) {
-                double e = 0.0;
                 unsigned long long a = 0;
-                for (int w = 0; w < (T + 31) / 32; ++w) {
-                    e += (double)s_eb[w];
-                    a += s_acc[w];
-                }
-                const int slot = ti % kSlots;
-                atomicAdd(&S->slot_eb[slot], e);
-                atomicAdd(&S->slot_acc[slot], a);
+                for (int w = 0; w < (T + 31) / 32; ++w) a += s_acc[w];
+                atomicAdd(&S->slot_acc[ti % kSlots], a);
             }
         }
 
-        if (MODE != kMoveOnly) {
+        if (MODE == kGridOnly) {
             const uint32_t buf = (MODE == kMoveGrid) ? (S->cur ^ 1u) : S->cur;
             uint32_t* cnt = S->counts[buf];
             const int64_t NC = S->n_cells;
@@ -357,13 +331,200 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
     }
 }
 
+// Linear chains, one warp per run of whole chains.  Each warp stages its
+// chains in its own slice of shared memory in a parity-split layout (for chain
+// cl: even beads at cl*L + b/2, odd beads at cl*L + h0 + b/2, h0 = ceil(L/2)),
+// so the lanes of a half-sweep read consecutive words, and the warp needs no
+// block barrier: load, even half-sweep, odd half-sweep, store, separated by
+// __syncwarp.  Results are identical to k_sweep (same trial, same keys).
+#ifndef SCMF_SWEEP_MIN_BLOCKS
+#define SCMF_SWEEP_MIN_BLOCKS 4
+#endif
+template <int MODE>
+__global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(const MoveTile* __restrict__ tiles, int n_tiles,
+                                                          int warp_beads) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    float* sx = reinterpret_cast<float*>(smem_raw) + (size_t)warp * 3 * warp_beads;
+    float* sy = sx + warp_beads;
+    float* sz = sy + warp_beads;
+    for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
+        const MoveTile t = tiles[ti];
+        SysDev* S = t.sys;
+        const ArchDev* Ap = t.arch;
+        const int L = Ap->length;
+        const int h0 = (L + 1) >> 1;
+        const int cpw = (t.n_chains + nwarps - 1) / nwarps;
+        const int c_begin = warp * cpw;
+        const int nch = min(cpw, t.n_chains - c_begin);
+        if (nch <= 0) continue;
+        const int nb = nch * L;
+        if (nb > warp_beads) {
+            if (lane == 0) atomicOr(&S->error_word, 2u);
+            continue;
+        }
+        MoveConsts c;
+        c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
+        c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
+        c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
+        const uint32_t len_magic = Ap->len_magic;
+        const int64_t g0 = t.bead0 + (int64_t)c_begin * L;
+        float* gx = S->x + g0;
+        float* gy = S->y + g0;
+        float* gz = S->z + g0;
+        for (int i = lane; i < nb; i += 32) {
+            const int cl = (int)div_magic((uint32_t)i, len_magic, L);
+            const int b = i - cl * L;
+            const int slot = cl * L + (b & 1) * h0 + (b >> 1);
+            sx[slot] = __ldcs(gx + i);
+            sy[slot] = __ldcs(gy + i);
+            sz[slot] = __ldcs(gz + i);
+        }
+        const uint8_t* __restrict__ types = Ap->types;
+        const int64_t NC = S->n_cells;
+        uint32_t* cnt = S->counts[MODE == kMoveGrid ? (S->cur ^ 1u) : S->cur];
+        const bool c16 = S->count16 != 0;
+        __syncwarp();
+        if (MODE != kGridOnly) {
+            const uint32_t step = S->step + 1u;
+            const uint32_t k0 = S->seed_lo, k1 = S->seed_hi;
+            const uint32_t my_cid = lane < nch ? __ldg(S->chain_id + t.chain0 + c_begin + lane) : 0u;
+            const float* __restrict__ omega = S->omega;
+            const float cc1 = S->cdeg[1], ac41 = S->ac4deg[1], cc2 = S->cdeg[2], ac42 = S->ac4deg[2];
+            unsigned nacc = 0;
+#pragma unroll 1
+            for (int col = 0; col < 2; ++col) {
+                const int half = col == 0 ? h0 : (L >> 1);
+                const uint32_t mg = Ap->color_magic[col];
+                const int items = nch * half;
+                const int own = col * h0, other = (1 - col) * h0;
+                // lanes of one iteration share the loop bound: every lane runs the
+                // shuffle below, inactive ones on a dummy item
+                for (int j0 = 0; j0 < items; j0 += 32) {
+                    const int j = j0 + lane;
+                    const bool act = j < items;
+                    const int jj = act ? j : 0;
+                    const int cl = (int)div_magic((uint32_t)jj, mg, half);
+                    const uint32_t gc = __shfl_sync(0xffffffffu, my_cid, cl & 31);
+                    if (!act) continue;
+                    const int k = jj - cl * half;
+                    const int b = 2 * k + col;
+                    const int base = cl * L;
+                    const int me = base + own + k;
+                    float qx[2], qy[2], qz[2];
+                    int deg = 0;
+                    if (b > 0) {
+                        const int q = base + other + k - 1 + col;
+                        qx[0] = sx[q];
+                        qy[0] = sy[q];
+                        qz[0] = sz[q];
+                        deg = 1;
+                    }
+                    if (b + 1 < L) {
+                        const int q = base + other + k + col;
+                        qx[deg] = sx[q];
+                        qy[deg] = sy[q];
+                        qz[deg] = sz[q];
+                        ++deg;
+                    }
+                    const int type = __ldg(types + b);
+                    const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1);
+                    float px, py, pz;
+                    int cell;
+                    const bool acc = trial<2>(c, sx[me], sy[me], sz[me], qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
+                                              deg == 2 ? ac42 : ac41, w, omega + (int64_t)type * NC, px, py, pz,
+                                              cell);
+                    if (acc) {
+                        sx[me] = px;
+                        sy[me] = py;
+                        sz[me] = pz;
+                    }
+                    nacc += acc ? 1u : 0u;
+                    if (MODE == kMoveGrid) {
+                        const int64_t idx = (int64_t)type * NC + cell;
+                        if (c16)
+                            atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16));
+                        else
+                            atomicAdd(cnt + idx, 1u);
+                    }
+                }
+                __syncwarp();
+            }
+            nacc = warp_sum(nacc);
+            if (lane == 0 && nacc) atomicAdd(&S->slot_acc[(ti * nwarps + warp) % kSlots], (unsigned long long)nacc);
+        }
+        if (MODE == kGridOnly) {
+            for (int i = lane; i < nb; i += 32) {
+                const int cl = (int)div_magic((uint32_t)i, len_magic, L);
+                const int b = i - cl * L;
+                const int slot = cl * L + (b & 1) * h0 + (b >> 1);
+                const int64_t idx = (int64_t)__ldg(types + b) * NC + cell_of(c, sx[slot], sy[slot], sz[slot]);
+                if (c16)
+                    atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16));
+                else
+                    atomicAdd(cnt + idx, 1u);
+            }
+        } else {
+            for (int i = lane; i < nb; i += 32) {
+                const int cl = (int)div_magic((uint32_t)i, len_magic, L);
+                const int b = i - cl * L;
+                const int slot = cl * L + (b & 1) * h0 + (b >> 1);
+                __stcs(gx + i, sx[slot]);
+                __stcs(gy + i, sy[slot]);
+                __stcs(gz + i, sz[slot]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------------ field
 __device__ __forceinline__ double read_clear(double* p) {
     return __longlong_as_double((long long)atomicExch(reinterpret_cast<unsigned long long*>(p), 0ull));
 }
 
-// Field of one cell for NT monomer types (NT = 0: runtime count, up to kMaxTypes).
-// Expression order matches the oracle's field_update().
+// omega of one cell from its counts (NT = 0: runtime type count, up to
+// kMaxTypes).  Expression order matches the oracle's field_update():
+// phi_S = n_S * scale, tot = sum_S phi_S (S ascending), then
+// SCMF0: w_T = (tot - 1) cf_TT + sum_{S != T} cf_TS (phi_T - phi_S)
+// literal: w_T = (tot - 1) cf_TT + sum_{S != T} cf_TS phi_S.
+template <int NT>
+__device__ __forceinline__ double omega_of_cell(int nt, const uint32_t* cnt, float scale, bool lit, bool upd, float* w,
+                                                const float* cf) {
+    constexpr int M = NT > 0 ? NT : kMaxTypes;
+    float phi[M];
+    float tot = 0.0f;
+#pragma unroll
+    for (int u = 0; u < M; ++u) {
+        if (u < nt) {
+            phi[u] = (float)cnt[u] * scale;
+            tot = tot + phi[u];
+        }
+    }
+    double ef = 0.0;
+#pragma unroll
+    for (int t = 0; t < M; ++t) {
+        if (t < nt) {
+            if (upd) {
+                float v = (tot - 1.0f) * cf[t + nt * t];
+#pragma unroll
+                for (int u = 0; u < M; ++u) {
+                    if (u < nt && u != t) {
+                        if (!lit)
+                            v = v + cf[t + nt * u] * (phi[t] - phi[u]);
+                        else
+                            v = v + cf[t + nt * u] * phi[u];
+                    }
+                }
+                w[t] = v;
+            }
+            ef += (double)w[t] * (double)cnt[t];
+        }
+    }
+    return ef;
+}
+
+// Scalar path: one cell (any count width, any alignment).
 template <int NT, bool FUSED>
 __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, float scale, bool lit, bool upd,
                                              bool c16, const uint32_t* src32, uint32_t* clr32, float* W,
@@ -372,45 +533,66 @@ __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, fl
     const int nt = NT > 0 ? NT : n;
     const uint16_t* src16 = reinterpret_cast<const uint16_t*>(src32);
     uint16_t* clr16 = reinterpret_cast<uint16_t*>(clr32);
-    float phi[M];
     uint32_t cnt[M];
-    float tot = 0.0f;
+    float w[M];
 #pragma unroll
     for (int u = 0; u < M; ++u) {
         if (u < nt) {
             cnt[u] = c16 ? (uint32_t)src16[u * NC + cell] : src32[u * NC + cell];
-            phi[u] = (float)cnt[u] * scale;
-            tot = tot + phi[u];
+            if (!upd) w[u] = W[u * NC + cell];
         }
+    }
+    const double ef = omega_of_cell<NT>(nt, cnt, scale, lit, upd, w, cf);
+#pragma unroll
+    for (int t = 0; t < M; ++t) {
+        if (t < nt) {
+            if (upd) W[t * NC + cell] = w[t];
+            if (FUSED) {
+                if (c16)
+                    clr16[t * NC + cell] = 0;
+                else
+                    clr32[t * NC + cell] = 0u;
+            }
+        }
+    }
+    return ef;
+}
+
+// Vector path: four consecutive cells with 16-byte loads and stores (32-bit
+// counts, n_cells and the tile start multiples of 4).
+template <int NT, bool FUSED>
+__device__ __forceinline__ double field_cells4(int64_t cell, int64_t NC, float scale, bool lit, bool upd,
+                                               const uint32_t* src32, uint32_t* clr32, float* W, const float* cf) {
+    uint4 cv[NT];
+    float4 wv[NT];
+#pragma unroll
+    for (int u = 0; u < NT; ++u) {
+        cv[u] = __ldcs(reinterpret_cast<const uint4*>(src32 + u * NC + cell));
+        if (!upd) wv[u] = *reinterpret_cast<const float4*>(W + u * NC + cell);
     }
     double ef = 0.0;
 #pragma unroll
-    for (int tt = 0; tt < M; ++tt) {
-        if (tt < nt) {
-            float w;
-            if (upd) {
-                w = (tot - 1.0f) * cf[tt + nt * tt];
+    for (int l = 0; l < 4; ++l) {
+        uint32_t cnt[NT];
+        float w[NT];
 #pragma unroll
-                for (int u = 0; u < M; ++u) {
-                    if (u < nt && u != tt) {
-                        if (!lit)
-                            w = w + cf[tt + nt * u] * (phi[tt] - phi[u]);
-                        else
-                            w = w + cf[tt + nt * u] * phi[u];
-                    }
-                }
-                W[tt * NC + cell] = w;
-            } else {
-                w = W[tt * NC + cell];
-            }
-            ef += (double)w * (double)cnt[tt];
-            if (FUSED) {
-                if (c16)
-                    clr16[tt * NC + cell] = 0;
-                else
-                    clr32[tt * NC + cell] = 0u;
-            }
+        for (int u = 0; u < NT; ++u) {
+            cnt[u] = l == 0 ? cv[u].x : l == 1 ? cv[u].y : l == 2 ? cv[u].z : cv[u].w;
+            w[u] = l == 0 ? wv[u].x : l == 1 ? wv[u].y : l == 2 ? wv[u].z : wv[u].w;
         }
+        ef += omega_of_cell<NT>(NT, cnt, scale, lit, upd, w, cf);
+#pragma unroll
+        for (int u = 0; u < NT; ++u) {
+            if (l == 0) wv[u].x = w[u];
+            else if (l == 1) wv[u].y = w[u];
+            else if (l == 2) wv[u].z = w[u];
+            else wv[u].w = w[u];
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < NT; ++u) {
+        if (upd) *reinterpret_cast<float4*>(W + u * NC + cell) = wv[u];
+        if (FUSED) *reinterpret_cast<uint4*>(clr32 + u * NC + cell) = make_uint4(0u, 0u, 0u, 0u);
     }
     return ef;
 }
@@ -439,8 +621,13 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
         float* W = S->omega;
         double ef = 0.0;
         const int64_t end = t.cell0 + t.n_cells;
-        for (int64_t cell = t.cell0 + tid; cell < end; cell += T)
-            ef += field_cell<NT, FUSED>(n, cell, NC, scale, lit, upd, c16, src32, clr32, W, cf);
+        if (NT > 0 && !c16 && (NC & 3) == 0 && (t.cell0 & 3) == 0 && (t.n_cells & 3) == 0) {
+            for (int64_t cell = t.cell0 + 4 * tid; cell < end; cell += 4 * T)
+                ef += field_cells4<(NT > 0 ? NT : 1), FUSED>(cell, NC, scale, lit, upd, src32, clr32, W, cf);
+        } else {
+            for (int64_t cell = t.cell0 + tid; cell < end; cell += T)
+                ef += field_cell<NT, FUSED>(n, cell, NC, scale, lit, upd, c16, src32, clr32, W, cf);
+        }
         ef = warp_sum(ef);
         if (lane == 0) s_ef[warp] = ef;
         __syncthreads();
@@ -460,15 +647,10 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
             S->e_field = e_f;
             if (FUSED) {
                 unsigned long long a = 0;
-                double e_b = 0.0;
-                for (int s = 0; s < kSlots; ++s) {
-                    a += atomicExch(&S->slot_acc[s], 0ull);
-                    e_b += read_clear(&S->slot_eb[s]);
-                }
+                for (int s = 0; s < kSlots; ++s) a += atomicExch(&S->slot_acc[s], 0ull);
                 S->last_accepts = a;
                 S->total_accepts += a;
                 S->total_moves += (unsigned long long)S->n_beads;
-                S->e_bond = e_b;
                 S->cur = cur ^ 1u;
                 S->step = sweep;
             }
@@ -482,16 +664,64 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
 __global__ void k_finalize_move(SysDev* S) {
     if (threadIdx.x != 0) return;
     unsigned long long a = 0;
-    double e_b = 0.0;
-    for (int s = 0; s < kSlots; ++s) {
-        a += atomicExch(&S->slot_acc[s], 0ull);
-        e_b += read_clear(&S->slot_eb[s]);
-    }
+    for (int s = 0; s < kSlots; ++s) a += atomicExch(&S->slot_acc[s], 0ull);
     S->last_accepts = a;
     S->total_accepts += a;
     S->total_moves += (unsigned long long)S->n_beads;
-    S->e_bond = e_b;
     S->step = S->step + 1u;
+}
+
+// Bond energy sum_bonds k |r_i - r_j|^2 of the current positions, each bond
+// once, accumulated into slot_eb; the last tile of the launch publishes it.
+__global__ void __launch_bounds__(256) k_bond_energy(const MoveTile* __restrict__ tiles, int n_tiles) {
+    __shared__ double s_e[32];
+    __shared__ int s_last;
+    const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
+        const MoveTile t = tiles[ti];
+        SysDev* S = t.sys;
+        const ArchDev* Ap = t.arch;
+        const int L = Ap->length;
+        const int nb = t.n_chains * L;
+        const float* X = S->x + t.bead0;
+        const float* Y = S->y + t.bead0;
+        const float* Z = S->z + t.bead0;
+        const float k = S->k;
+        double e = 0.0;
+        for (int i = tid; i < nb; i += T) {
+            const int cl = (int)div_magic((uint32_t)i, Ap->len_magic, L);
+            const int b = i - cl * L;
+            const BeadInfo bi = Ap->beads[b];
+            for (int d = 0; d < bi.deg; ++d) {
+                const int j = bi.nbr[d];
+                if (j <= b) continue;
+                const int jj = cl * L + j;
+                const float ex = X[i] - X[jj], ey = Y[i] - Y[jj], ez = Z[i] - Z[jj];
+                e += (double)k * (double)(ex * ex + ey * ey + ez * ez);
+            }
+        }
+        e = warp_sum(e);
+        if (lane == 0) s_e[warp] = e;
+        __syncthreads();
+        if (tid == 0) {
+            double a = 0.0;
+            for (int w = 0; w < (T + 31) / 32; ++w) a += s_e[w];
+            atomicAdd(&S->slot_eb[ti % kSlots], a);
+            __threadfence();
+            s_last = (atomicAdd(&S->field_done, 1u) == (unsigned)t.n_tiles_sys - 1u);
+        }
+        __syncthreads();
+        if (s_last && tid == 0) {
+            __threadfence();
+            double a = 0.0;
+            for (int s = 0; s < kSlots; ++s) a += read_clear(&S->slot_eb[s]);
+            S->e_bond = a;
+            S->e_bond_step = S->step + 1u;
+            S->field_done = 0u;
+            __threadfence();
+        }
+        __syncthreads();
+    }
 }
 
 // ------------------------------------------------------------- transposes
@@ -588,22 +818,31 @@ int configure_kernels() {
     cudaError_t e = allow_smem<kMoveOnly, false>(bytes);
     if (e == cudaSuccess) e = allow_smem<kMoveGrid, false>(bytes);
     if (e == cudaSuccess) e = allow_smem<kGridOnly, false>(bytes);
-    if (e == cudaSuccess) e = allow_smem<kMoveOnly, true>(bytes);
-    if (e == cudaSuccess) e = allow_smem<kMoveGrid, true>(bytes);
-    if (e == cudaSuccess) e = allow_smem<kGridOnly, true>(bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep_linear<kMoveOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep_linear<kMoveGrid>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep_linear<kGridOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) done = 1;
     return (int)e;
 }
 
 template <int MODE>
 static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, LaunchShape sh, cudaStream_t st) {
-    const size_t smem = sweep_smem_bytes(mtb, ml);
-    if (mtb > kMaxTileBeads || ml > kMaxLength || sh.threads > 256) return (int)cudaErrorInvalidValue;
+    if (mtb > kMaxTileBeads || ml > kMaxLength || sh.threads > 256 || sh.threads < 32) return (int)cudaErrorInvalidValue;
     const int blocks = sh.blocks > 0 ? sh.blocks : n_tiles;
-    if (sh.linear)
-        k_sweep<MODE, true><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml);
-    else
+    if (sh.linear) {
+        // per-warp slice: ceil(chains per tile / warps) chains of the longest length
+        const int nw = sh.threads / 32;
+        const int wb = ((sh.max_chains + nw - 1) / nw) * ml;
+        const size_t smem = (size_t)nw * 3 * wb * sizeof(float);
+        if (smem > sweep_smem_bytes(kMaxTileBeads, kMaxLength)) return (int)cudaErrorInvalidValue;
+        k_sweep_linear<MODE><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, wb);
+    } else {
+        const size_t smem = sweep_smem_bytes(mtb, ml);
         k_sweep<MODE, false><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml);
+    }
     return (int)cudaGetLastError();
 }
 
@@ -637,6 +876,12 @@ int launch_field(bool fused, int force_update, const FieldTile* tiles, int n_til
         launch_field_t<true>(sh.n_types, tiles, n_tiles, force_update, blocks, threads, st);
     else
         launch_field_t<false>(sh.n_types, tiles, n_tiles, force_update, blocks, threads, st);
+    return (int)cudaGetLastError();
+}
+
+int launch_bond_energy(const MoveTile* tiles, int n_tiles, SysDev*, LaunchShape sh, void* stream) {
+    if (n_tiles <= 0) return 0;
+    k_bond_energy<<<n_tiles, sh.threads > 256 ? 256 : sh.threads, 0, (cudaStream_t)stream>>>(tiles, n_tiles);
     return (int)cudaGetLastError();
 }
 

@@ -33,9 +33,10 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
     return c;
 }
 
-// Odd multiples of 2^-24 in (0,1); exact in FP32.
+// Uniform in (0, 1] from bits 9..31: 2 - 1.m with the 23 bits as mantissa
+// (exact in FP32; no integer-to-float conversion).
 __device__ __forceinline__ float u01(uint32_t w) {
-    return __uint2float_rn((w >> 8) | 1u) * 0x1p-24f;
+    return __fsub_rn(2.0f, __uint_as_float(0x3F800000u | (w >> 9)));
 }
 
 // log(x) for normal x > 0.  x = 2^e m with m in [sqrt(1/2), sqrt(2));
@@ -113,10 +114,17 @@ __device__ __forceinline__ uint32_t accept_word(uint4 w) {
     return ((w.y & 0xFFu) << 24) | ((w.z & 0xFFu) << 16) | ((w.w & 0xFFu) << 8);
 }
 
-// floor(x * inv_d) mod n, in [0, n).  FP32 restatement of the periodic fold in
-// coord_to_index_unified_high (device_function.cu:313-360).
+// floor(x * inv_d) mod n, in [0, n), for |x * inv_d| < 2^22 (beyond that the
+// index stays in [0, n) but need not be the floor).  FP32 restatement of the
+// periodic fold in coord_to_index_unified_high (device_function.cu:313-360).
+// floor(t) for |t| < 2^22 without a conversion instruction: t + 1.5*2^23
+// rounded down is 1.5*2^23 + floor(t) exactly, read back from the mantissa.
+// One box away is folded with selects; the general modulo only runs for
+// coordinates more than one box length outside the primary box.
 __device__ __forceinline__ int fold(float x, float inv_d, int n) {
-    int i = __float2int_rd(__fmul_rn(x, inv_d));
+    int i = __float_as_int(__fadd_rd(__fmul_rn(x, inv_d), 0x1.8p23f)) - 0x4B400000;
+    i = i < 0 ? i + n : i;
+    i = i >= n ? i - n : i;
     if ((unsigned)i >= (unsigned)n) {
         i %= n;
         if (i < 0) i += n;

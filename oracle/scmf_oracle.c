@@ -60,8 +60,8 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
-/* Uniform on the odd multiples of 2^-24 in (0,1): exact in float. */
-float orc_u01(uint32_t w) { return (float)((w >> 8) | 1u) * 0x1p-24f; }
+/* Uniform in (0, 1] from bits 9..31: 2 - 1.m with the 23 bits as mantissa. */
+float orc_u01(uint32_t w) { return 2.0f - u2f(0x3F800000u | (w >> 9)); }
 
 /* Natural log for normal positive floats: x = 2^e m, m in [sqrt(1/2), sqrt(2)),
  * log m = log1p(t) = t + t^2 Q(t), t = m - 1 (exact), Q of degree 8 fitted by
@@ -138,8 +138,9 @@ uint32_t orc_accept_word(const uint32_t w[4]) {
     return ((w[1] & 0xFFu) << 24) | ((w[2] & 0xFFu) << 16) | ((w[3] & 0xFFu) << 8);
 }
 
-/* Periodic fold of one coordinate to a cell index in [0, n): floor(x/dx) mod n.
- * Restates coord_to_index_unified_high (device_function.cu:313-360) in FP32. */
+/* Periodic fold of one coordinate to a cell index in [0, n): floor(x/dx) mod n
+ * (for |x/dx| < 2^22, the range the kernels support).  Restates
+ * coord_to_index_unified_high (device_function.cu:313-360) in FP32. */
 int orc_fold(float x, float inv_d, int n) {
     float t = x * inv_d;
     int i = (int)floorf(t);
@@ -176,12 +177,12 @@ struct orc_system {
     int64_t n_beads, n_cells;
     /* derived float constants */
     float k, k2, A, R, inv_dx, inv_dy, inv_dz, scale, flx, fly, flz;
+    float cdeg[ORC_MAX_DEG + 1], ac4deg[ORC_MAX_DEG + 1];   /* c = k2 deg, A c / 4 */
     float cf[ORC_MAX_TYPES * ORC_MAX_TYPES];
     /* state */
     float *x, *y, *z;
     uint32_t* counts;
     float* omega;
-    double* chain_ebond;
     uint32_t* chain_acc;
     uint64_t step;
     orc_stats st;
@@ -266,6 +267,10 @@ int orc_finalize(orc_system* s) {
     s->k2 = (float)(2.0 * s->kd);
     s->A = (float)s->ad;
     s->R = (float)sqrt(2.0 * s->ad);
+    for (int d = 0; d <= ORC_MAX_DEG; ++d) {
+        s->cdeg[d] = s->k2 * (float)d;
+        s->ac4deg[d] = (s->A * s->cdeg[d]) * 0.25f;
+    }
     s->inv_dx = (float)((double)s->nx / s->lx);
     s->inv_dy = (float)((double)s->ny / s->ly);
     s->inv_dz = (float)((double)s->nz / s->lz);
@@ -285,7 +290,6 @@ int orc_finalize(orc_system* s) {
     s->z = (float*)calloc(nb > 0 ? nb : 1, sizeof(float));
     s->counts = (uint32_t*)calloc(s->n_cells * n, sizeof(uint32_t));
     s->omega = (float*)calloc(s->n_cells * n, sizeof(float));
-    s->chain_ebond = (double*)calloc(nc > 0 ? nc : 1, sizeof(double));
     s->chain_acc = (uint32_t*)calloc(nc > 0 ? nc : 1, sizeof(uint32_t));
     s->finalized = 1;
     return 0;
@@ -297,7 +301,7 @@ void orc_destroy(orc_system* s) {
         free(s->arch[a].type); free(s->arch[a].deg); free(s->arch[a].nbr); free(s->arch[a].color);
     }
     free(s->x); free(s->y); free(s->z); free(s->counts); free(s->omega);
-    free(s->chain_ebond); free(s->chain_acc);
+    free(s->chain_acc);
     free(s);
 }
 
@@ -315,7 +319,7 @@ void orc_get_coords(const orc_system* s, float* p) {
 void orc_get_counts(const orc_system* s, uint32_t* out) { memcpy(out, s->counts, sizeof(uint32_t) * s->n_cells * s->n_types); }
 void orc_get_omega(const orc_system* s, float* out) { memcpy(out, s->omega, sizeof(float) * s->n_cells * s->n_types); }
 void orc_set_omega(orc_system* s, const float* in) { memcpy(s->omega, in, sizeof(float) * s->n_cells * s->n_types); }
-void orc_get_stats(const orc_system* s, orc_stats* out) { *out = s->st; out->step = s->step; }
+
 
 static inline void key_of(const orc_system* s, uint32_t key[2]) {
     key[0] = (uint32_t)s->seed; key[1] = (uint32_t)(s->seed >> 32);
@@ -372,67 +376,111 @@ static inline int64_t cell_of(const orc_system* s, float x, float y, float z) {
     return (int64_t)ix + (int64_t)s->nx * ((int64_t)iy + (int64_t)s->ny * iz);
 }
 
-/* One smart-MC trial of bead b (device_function.cu:637-717, 562-588, 444-454).
- * Returns 1 if accepted; adds to *eb the bond energy k |r_b - r_j|^2 of the
- * final position of b for every neighbour j of lower colour (final by then),
- * so every bond is counted once per sweep. */
-static inline int move_bead(const orc_system* s, const orc_arch* a, uint32_t gc, int b,
-                            float* X, float* Y, float* Z, const uint32_t key[2], uint32_t step, float* eb) {
+/* Bonded energy change plus smart-MC correction of a trial displacement d of
+ * a bead with deg harmonic bonds, transcribed literally from the reference:
+ * calc_delta_bonded_energy_arr (device_function.cu:509-561) + the smc_deltaE
+ * of trial_move_smc_arr (device_function.cu:700-713), in FP64 like the
+ * reference.  Used by the tests to check the closed form below. */
+double orc_dE_literal(int deg, const float* q, const float* p, const float* d, double k, double A) {
+    double f[3] = {0, 0, 0}, nf[3] = {0, 0, 0}, deb = 0.0;
+    for (int j = 0; j < deg; ++j)
+        for (int a = 0; a < 3; ++a) f[a] += ((double)q[3 * j + a] - p[a]) * 2.0 * k;
+    for (int j = 0; j < deg; ++j) {
+        double o2 = 0, e2 = 0;
+        for (int a = 0; a < 3; ++a) {
+            double o = (double)p[a] - q[3 * j + a], e = o + d[a];
+            o2 += o * o;
+            e2 += e * e;
+            nf[a] += ((double)q[3 * j + a] - ((double)p[a] + d[a])) * 2.0 * k;
+        }
+        deb += k * (e2 - o2);
+    }
+    double smc = 0.5 * ((nf[0] + f[0]) * d[0] + (nf[1] + f[1]) * d[1] + (nf[2] + f[2]) * d[2]);
+    smc += 0.25 * A * (nf[0] * nf[0] + nf[1] * nf[1] + nf[2] * nf[2] - f[0] * f[0] - f[1] * f[1] - f[2] * f[2]);
+    return deb + smc;
+}
+
+/* The same quantity in closed form.  With f = 2k sum_j (q_j - p) the force at
+ * p, the force at p + d is f - c d (c = 2k deg), and the bonded change plus the
+ * smart-MC term reduce exactly to (A c / 4) (c |d|^2 - 2 f.d).  This is what
+ * both the oracle and the kernels evaluate, in FP32 with explicit fmaf. */
+static inline float dE_closed(float c, float ac4, float fx, float fy, float fz, float dx, float dy, float dz) {
+    float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float fd = fmaf(fx, dx, fmaf(fy, dy, fz * dz));
+    return ac4 * fmaf(c, d2, -2.0f * fd);
+}
+
+float orc_dE_closed(int deg, const float* q, const float* p, const float* d, float k2, float A) {
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    for (int j = 0; j < deg; ++j) {
+        fx = fmaf(q[3 * j] - p[0], k2, fx);
+        fy = fmaf(q[3 * j + 1] - p[1], k2, fy);
+        fz = fmaf(q[3 * j + 2] - p[2], k2, fz);
+    }
+    float c = k2 * (float)deg;
+    return dE_closed(c, (A * c) * 0.25f, fx, fy, fz, d[0], d[1], d[2]);
+}
+
+/* One smart-MC trial of bead b (device_function.cu:637-717, 562-588, 444-454)
+ * with the Gaussian triple (n0, n1, n2) and the Metropolis word aw: force from
+ * the bonded neighbours (ascending order), displacement d = A f + R xi, energy
+ * change omega[new cell] - omega[old cell] + the closed form above, Metropolis
+ * test.  Returns 1 if accepted. */
+static inline int move_bead(const orc_system* s, const orc_arch* a, int b, float* X, float* Y, float* Z,
+                            float n0, float n1, float n2, uint32_t aw) {
     const int* nb = a->nbr + b * ORC_MAX_DEG;
     const int deg = a->deg[b];
-    const float k = s->k, k2 = s->k2, A = s->A, R = s->R;
-    float x = X[b], y = Y[b], z = Z[b];
+    const float k2 = s->k2, A = s->A, R = s->R;
+    const float x = X[b], y = Y[b], z = Z[b];
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
     for (int d = 0; d < deg; ++d) {
         int j = nb[d];
-        fx = fx + (X[j] - x) * k2;
-        fy = fy + (Y[j] - y) * k2;
-        fz = fz + (Z[j] - z) * k2;
+        fx = fmaf(X[j] - x, k2, fx);
+        fy = fmaf(Y[j] - y, k2, fy);
+        fz = fmaf(Z[j] - z, k2, fz);
     }
+    const float dx = fmaf(A, fx, R * n0);
+    const float dy = fmaf(A, fy, R * n1);
+    const float dz = fmaf(A, fz, R * n2);
+    const float px = x + dx, py = y + dy, pz = z + dz;
+    const float c = s->cdeg[deg], ac4 = s->ac4deg[deg];
+    const int t = a->type[b];
+    const float* W = s->omega + (int64_t)t * s->n_cells;
+    const float w_old = W[cell_of(s, x, y, z)];
+    const float w_new = W[cell_of(s, px, py, pz)];
+    const float dE = (w_new - w_old) + dE_closed(c, ac4, fx, fy, fz, dx, dy, dz);
+    /* Metropolis: accept if dE < 0, else if log(u) < -dE.  log(u) >= -23 ln2
+     * > -17 for every u the generator yields, so dE >= 17 always rejects. */
+    int acc;
+    if (dE < 0.0f) acc = 1;
+    else if (dE < 17.0f) acc = orc_logf(orc_u01(aw)) < -dE;
+    else acc = 0;
+    if (acc) { X[b] = px; Y[b] = py; Z[b] = pz; }
+    return acc;
+}
+
+/* One trial of bead b: its Philox block (chain, b, step, 0) gives the three
+ * normals and the Metropolis word. */
+static inline int move_single(const orc_system* s, const orc_arch* a, uint32_t gc, int b,
+                              float* X, float* Y, float* Z, const uint32_t key[2], uint32_t step) {
     uint32_t ctr[4] = {gc, (uint32_t)b, step, 0u}, w[4];
     orc_philox4x32_10(ctr, key, w);
     float n0, n1, n2;
     orc_normals3(w, &n0, &n1, &n2);
-    float dx = A * fx + R * n0;
-    float dy = A * fy + R * n1;
-    float dz = A * fz + R * n2;
-    float px = x + dx, py = y + dy, pz = z + dz;
-    float nfx = 0.0f, nfy = 0.0f, nfz = 0.0f;
-    float deb = 0.0f;
-    float o2s[ORC_MAX_DEG], e2s[ORC_MAX_DEG];
-    for (int d = 0; d < deg; ++d) {
-        int j = nb[d];
-        float qx = X[j], qy = Y[j], qz = Z[j];
-        nfx = nfx + (qx - px) * k2;
-        nfy = nfy + (qy - py) * k2;
-        nfz = nfz + (qz - pz) * k2;
-        float ox = x - qx, oy = y - qy, oz = z - qz;
-        float ex = ox + dx, ey = oy + dy, ez = oz + dz;
-        float o2 = ox * ox + oy * oy + oz * oz;
-        float e2 = ex * ex + ey * ey + ez * ez;
-        o2s[d] = o2;
-        e2s[d] = e2;
-        deb = deb + k * (e2 - o2);
-    }
-    float smc = 0.5f * ((nfx + fx) * dx + (nfy + fy) * dy + (nfz + fz) * dz)
-              + 0.25f * A * (nfx * nfx + nfy * nfy + nfz * nfz - fx * fx - fy * fy - fz * fz);
-    const int t = a->type[b];
-    const float* W = s->omega + (int64_t)t * s->n_cells;
-    float w_old = W[cell_of(s, x, y, z)];
-    float w_new = W[cell_of(s, px, py, pz)];
-    float dE = (w_new - w_old) + deb;
-    dE = dE + smc;
-    /* Metropolis: accept if dE < 0, else if log(u) < -dE.  log(u) >= -24 ln2
-     * > -17 for every u the generator yields, so dE >= 17 always rejects. */
-    int acc;
-    if (dE < 0.0f) acc = 1;
-    else if (dE < 17.0f) acc = orc_logf(orc_u01(orc_accept_word(w))) < -dE;
-    else acc = 0;
-    if (acc) { X[b] = px; Y[b] = py; Z[b] = pz; }
-    const int cb = a->color[b];
-    for (int d = 0; d < deg; ++d)
-        if (a->color[nb[d]] < cb) *eb += k * (acc ? e2s[d] : o2s[d]);
-    return acc;
+    return move_bead(s, a, b, X, Y, Z, n0, n1, n2, orc_accept_word(w));
+}
+
+/* Bond energy of one chain, each bond once: sum k |r_i - r_j|^2. */
+static double chain_bond_energy(const orc_system* s, const orc_arch* a, const float* X, const float* Y, const float* Z) {
+    double e = 0.0;
+    for (int i = 0; i < a->length; ++i)
+        for (int d = 0; d < a->deg[i]; ++d) {
+            int j = a->nbr[i * ORC_MAX_DEG + d];
+            if (j <= i) continue;
+            float ex = X[i] - X[j], ey = Y[i] - Y[j], ez = Z[i] - Z[j];
+            e += (double)s->k * (double)(ex * ex + ey * ey + ez * ez);
+        }
+    return e;
 }
 
 static void sweep_moves(orc_system* s, uint32_t step) {
@@ -445,20 +493,17 @@ static void sweep_moves(orc_system* s, uint32_t step) {
             float* X = s->x + b0; float* Y = s->y + b0; float* Z = s->z + b0;
             uint32_t gc = (uint32_t)(ar->chain_base + c);
             uint32_t nacc = 0;
-            float eb = 0.0f;
             for (int col = 0; col < ar->n_colors; ++col)
                 for (int b = 0; b < ar->length; ++b)
-                    if (ar->color[b] == col) nacc += (uint32_t)move_bead(s, ar, gc, b, X, Y, Z, key, step, &eb);
+                    if (ar->color[b] == col) nacc += (uint32_t)move_single(s, ar, gc, b, X, Y, Z, key, step);
             s->chain_acc[ar->chain_base + c] = nacc;
-            s->chain_ebond[ar->chain_base + c] = (double)eb;
         }
     }
-    uint64_t acc = 0; double eb = 0.0;
-    for (int c = 0; c < s->n_chains; ++c) { acc += s->chain_acc[c]; eb += s->chain_ebond[c]; }
+    uint64_t acc = 0;
+    for (int c = 0; c < s->n_chains; ++c) acc += s->chain_acc[c];
     s->st.last_accepts = acc;
     s->st.total_accepts += acc;
     s->st.total_moves += (uint64_t)s->n_beads;
-    s->st.e_bond = eb;
 }
 
 void orc_smc_move(orc_system* s, int n) {
@@ -530,4 +575,20 @@ void orc_step(orc_system* s, int n) {
         int upd = (s->field_rule == 1) || (s->step % 10 != 0);
         field_update(s, upd);
     }
+}
+
+/* Statistics; the bond energy is that of the current positions, computed on
+ * demand (as the engine does). */
+void orc_get_stats(const orc_system* s, orc_stats* out) {
+    *out = s->st;
+    out->step = s->step;
+    double eb = 0.0;
+    for (int a = 0; a < s->n_arch; ++a) {
+        const orc_arch* ar = &s->arch[a];
+        for (int c = 0; c < ar->n_chains; ++c) {
+            int64_t b0 = ar->bead_base + (int64_t)c * ar->length;
+            eb += chain_bond_energy(s, ar, s->x + b0, s->y + b0, s->z + b0);
+        }
+    }
+    out->e_bond = eb;
 }

@@ -81,6 +81,8 @@ void  orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2);
 float orc_u01(uint32_t w);
 uint32_t orc_accept_word(const uint32_t w[4]);
 int   orc_fold(float x, float inv_d, int n);
+double orc_dE_literal(int deg, const float* q, const float* p, const float* d, double k, double A);
+float  orc_dE_closed(int deg, const float* q, const float* p, const float* d, float k2, float A);
 
 #ifdef __cplusplus
 }
