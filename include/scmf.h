@@ -175,6 +175,26 @@ scmf_status scmf_get_stats(const scmf_system* sys, scmf_stats* out);
 scmf_status scmf_debug_math(uint32_t key_lo, uint32_t key_hi, int32_t n, uint32_t* words, float* logs,
                             float* sines, float* cosines, float* normals);
 
+/* Field update that allocates nothing.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc: code that must not allocate while
+ * it runs (work replayed inside a stream capture owned by someone else, a
+ * latency-critical loop where an allocation could stall), or an application
+ * that owns every byte of device memory and passes only pointers to its own
+ * buffers.  It computes omega (SCMF0 or literal, as scmf_update_omega_fields_scmf0)
+ * from caller-owned device counts d_counts[n_types*n_cells] into caller-owned
+ * d_omega, and the field energy sum_T sum_cells omega_T n_T into the device
+ * double *d_energy, enqueued on `stream`.  Its only scratch, the per-tile
+ * energy partials, is a fixed array in the library's device memory: at most
+ * 8,388,608 cells (2048 tiles of 4096); larger grids are rejected with
+ * SCMF_E_INVALID.  Every GPU that loads the library holds that 16 KiB until
+ * the process exits.  The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the array and each overwrites it: calls that overlap on the
+ * GPU (different streams, or devices sharing one context) race. */
+scmf_status scmf_update_omega_noalloc(const uint32_t* d_counts, float* d_omega, int32_t n_types, int64_t n_cells,
+                                      double field_scaling, const double* xn, int32_t reference_nbeads,
+                                      int32_t hamiltonian, double* d_energy, void* stream);
+
 /* --------------------------------------------------------------- output */
 /* density_<step>.dat writer (io_out_density, io.cpp:4-56).  path NULL uses the
  * reference's file name rule in the current directory. */

@@ -172,6 +172,20 @@ size_t system_device_bytes(const scmf_spec& s) {
     return b;
 }
 
+void field_coefficients(int n, const double* xn, int nref, int hamiltonian, float* cf) {
+    const double inv_n = 1.0 / (double)nref;
+    for (int i = 0; i < kMaxTypes * kMaxTypes; ++i) cf[i] = 0.0f;
+    for (int t = 0; t < n; ++t)
+        for (int u = 0; u < n; ++u) {
+            const double v = xn[t + n * u];
+            float c;
+            if (t == u) c = (float)(v * inv_n);
+            else if (hamiltonian == SCMF_HAM_SCMF0) c = (float)(-0.5 * v * inv_n);
+            else c = (float)(v * inv_n);
+            cf[t + n * u] = c;
+        }
+}
+
 void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d) {
     d->n_types = s.n_types;
     d->nx = s.nx; d->ny = s.ny; d->nz = s.nz;
@@ -191,18 +205,7 @@ void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d) {
         d->cdeg[g] = d->k2 * (float)g;
         d->ac4deg[g] = (d->A * d->cdeg[g]) * 0.25f;
     }
-    const double inv_n = 1.0 / (double)s.p.reference_nbeads;
-    const int n = s.n_types;
-    for (int i = 0; i < kMaxTypes * kMaxTypes; ++i) d->cf[i] = 0.0f;
-    for (int t = 0; t < n; ++t)
-        for (int u = 0; u < n; ++u) {
-            const double v = s.xn[t + n * u];
-            float c;
-            if (t == u) c = (float)(v * inv_n);
-            else if (s.p.hamiltonian == SCMF_HAM_SCMF0) c = (float)(-0.5 * v * inv_n);
-            else c = (float)(v * inv_n);
-            d->cf[t + n * u] = c;
-        }
+    field_coefficients(s.n_types, s.xn.data(), s.p.reference_nbeads, s.p.hamiltonian, d->cf);
     d->hamiltonian = s.p.hamiltonian;
     d->field_rule = s.p.field_rule;
     d->count16 = s.p.count_bits == 16 ? 1 : 0;

@@ -19,6 +19,8 @@
 #pragma once
 #include <stdint.h>
 
+#include "scmf.h"
+
 namespace scmf {
 
 constexpr int kMaxTypes = 8;
@@ -128,6 +130,11 @@ int launch_soa_to_aos(float* aos, const SysDev* sys, const ArchDev* arch, int n_
                       void* stream);
 int launch_unpack_counts16(const SysDev* sys, uint32_t* out, int64_t n, void* stream);
 size_t sweep_smem_bytes(int max_tile_beads, int max_length);
+// Field coefficients cf[t + n*s] in FP32 from xn[t + n*s] (double): diagonal
+// xn/N_ref; off-diagonal -xn/(2 N_ref) (SCMF0) or xn/N_ref (literal).
+void field_coefficients(int n, const double* xn, int nref, int hamiltonian, float* cf);
+// Sets the thread's last-error message (scmf_engine.cpp); returns code.
+scmf_status fail(scmf_status code, const char* fmt, ...);
 int configure_kernels();
 int launch_debug_math(uint32_t k0, uint32_t k1, int n, uint32_t* words, float* logs, float* sines, float* cosines,
                       float* normals, void* stream);

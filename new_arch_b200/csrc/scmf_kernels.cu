@@ -15,6 +15,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
+#include "scmf.h"
+
 #include "scmf_internal.h"
 #include "scmf_math.cuh"
 
@@ -909,3 +913,127 @@ int launch_unpack_counts16(const SysDev* sys, uint32_t* out, int64_t n, void* st
 }
 
 }  // namespace scmf
+
+// ---------------------------------------------------------------------------
+// Field update without allocation.
+//
+// For callers that cannot call cudaMalloc (code that runs where allocation is
+// forbidden or must not stall, such as a step that is replayed inside someone
+// else's captured stream work, or an embedding application that owns all
+// device memory and hands out only pointers to its own buffers), the omega
+// update of caller-owned counts into caller-owned omega is offered with its
+// only scratch, the per-tile partial sums of the field energy, held in a fixed
+// array in this library's device memory.  Every GPU that loads the library
+// holds that array (kNoAllocMaxTiles doubles, 16 KiB) until the process exits.
+namespace scmf {
+
+constexpr int kNoAllocTileCells = 4096;
+constexpr int kNoAllocMaxTiles = 2048;  // n_cells <= 2048 * 4096 = 8,388,608
+
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxTiles];
+
+struct FieldParams {
+    int64_t n_cells;
+    float scale;
+    int n_types;
+    int lit;
+    float cf[kMaxTypes * kMaxTypes];
+};
+
+// One tile of kNoAllocTileCells cells per block: omega of every cell and the
+// tile's field energy sum_T omega_T n_T into partials[tile] (no atomics).
+__global__ void __launch_bounds__(256) k_field_noalloc(const uint32_t* __restrict__ counts, float* __restrict__ omega,
+                                                        FieldParams p, double* __restrict__ partials) {
+    __shared__ double s_ef[32];
+    __shared__ float cf[kMaxTypes * kMaxTypes];
+    const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < kMaxTypes * kMaxTypes; i += T) cf[i] = p.cf[i];
+    __syncthreads();
+    const int64_t c0 = (int64_t)blockIdx.x * kNoAllocTileCells;
+    const int64_t c1 = min(c0 + (int64_t)kNoAllocTileCells, p.n_cells);
+    double ef = 0.0;
+    for (int64_t cell = c0 + tid; cell < c1; cell += T)
+        ef += field_cell<0, false>(p.n_types, cell, p.n_cells, p.scale, p.lit != 0, true, false, counts, nullptr,
+                                   omega, cf);
+    ef = warp_sum(ef);
+    if (lane == 0) s_ef[warp] = ef;
+    __syncthreads();
+    if (tid == 0) {
+        double e = 0.0;
+        for (int w = 0; w < (T + 31) / 32; ++w) e += s_ef[w];
+        partials[blockIdx.x] = e;
+    }
+}
+
+// Sum of the tile partials in a fixed order (one block).
+__global__ void __launch_bounds__(256) k_sum_partials(const double* __restrict__ partials, int n,
+                                                       double* __restrict__ out) {
+    __shared__ double s[256];
+    double e = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) e += partials[i];
+    s[threadIdx.x] = e;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
+// Device address of the scratch array, looked up once per device (with that
+// device current) and cached.  The host-side name of a __device__ variable is
+// only a stand-in for it and must never be passed to a kernel.
+static double* noalloc_scratch(int device, cudaError_t* err) {
+    static std::mutex mu;
+    static double* addr[64] = {nullptr};
+    if (device < 0 || device >= 64) {
+        *err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> g(mu);
+    if (!addr[device]) {
+        void* p = nullptr;
+        *err = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (*err != cudaSuccess) return nullptr;
+        addr[device] = static_cast<double*>(p);
+    }
+    *err = cudaSuccess;
+    return addr[device];
+}
+
+}  // namespace scmf
+
+// The entry point (declared in include/scmf.h).
+extern "C" scmf_status scmf_update_omega_noalloc(const uint32_t* d_counts, float* d_omega, int32_t n_types,
+                                                 int64_t n_cells, double field_scaling, const double* xn,
+                                                 int32_t reference_nbeads, int32_t hamiltonian, double* d_energy,
+                                                 void* stream) {
+    using namespace scmf;
+    if (!d_counts || !d_omega || !xn || !d_energy) return fail(SCMF_E_INVALID, "NULL argument");
+    if (n_types < 1 || n_types > kMaxTypes) return fail(SCMF_E_INVALID, "n_types %d not in [1,%d]", n_types, kMaxTypes);
+    if (n_cells < 1) return fail(SCMF_E_INVALID, "n_cells must be positive");
+    if (n_cells > (int64_t)kNoAllocMaxTiles * kNoAllocTileCells)
+        return fail(SCMF_E_INVALID,
+                    "n_cells %lld exceeds the %lld cells the fixed scratch of the allocation-free field update covers",
+                    (long long)n_cells, (long long)kNoAllocMaxTiles * kNoAllocTileCells);
+    if (reference_nbeads < 1) return fail(SCMF_E_INVALID, "reference_nbeads must be >= 1");
+    if (hamiltonian != SCMF_HAM_SCMF0 && hamiltonian != SCMF_HAM_LITERAL) return fail(SCMF_E_INVALID, "unknown hamiltonian");
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return fail(SCMF_E_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    double* scratch = noalloc_scratch(device, &e);
+    if (!scratch) return fail(SCMF_E_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    FieldParams p{};
+    p.n_cells = n_cells;
+    p.scale = (float)field_scaling;
+    p.n_types = n_types;
+    p.lit = hamiltonian == SCMF_HAM_LITERAL;
+    field_coefficients(n_types, xn, reference_nbeads, hamiltonian, p.cf);
+    const int tiles = (int)((n_cells + kNoAllocTileCells - 1) / kNoAllocTileCells);
+    cudaStream_t st = (cudaStream_t)stream;
+    k_field_noalloc<<<tiles, 256, 0, st>>>(d_counts, d_omega, p, scratch);
+    k_sum_partials<<<1, 256, 0, st>>>(scratch, tiles, d_energy);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(SCMF_E_CUDA, "launch: %s", cudaGetErrorString(e));
+    return SCMF_OK;
+}
