@@ -70,15 +70,15 @@ scmf_status regrid(scmf_system* s) {
     LaunchShape sh = s->plan.move_shape();
     sh.blocks = 0;
     CKL(launch_sweep(kGridOnly, s->plan.d_move, s->plan.n_move, s->plan.max_tile_beads, s->plan.max_length, sh,
-                     s->stream));
+                     s->plan.d_acc, s->stream));
     return SCMF_OK;
 }
 
 scmf_status field_now(scmf_system* s) {
     LaunchShape sh = s->plan.field_shape();
     sh.blocks = 0;
-    CKL(launch_field(false, 1, s->plan.d_field, s->plan.n_field, sh, s->stream));
-    return SCMF_OK;
+    CKL(launch_field(false, 1, s->plan.d_field, s->plan.n_field, sh, s->plan.d_ef, s->stream));
+    return s->plan.enqueue_close(kCloseField, s->stream);
 }
 
 scmf_status ensure_aos(scmf_system* s) {
@@ -307,6 +307,7 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
             d.color_magic[c] = magic_for(nc);
         }
         d.len_magic = magic_for((uint32_t)a.length);
+        d.tpc_magic = magic_for((uint32_t)((a.length + 1) / 2));
         d.n_chains = a.n_chains;
         d.chain_base = a.chain_base;
         d.bead_base = a.bead_base;
@@ -422,9 +423,12 @@ scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float*
     const LaunchShape fs = p.field_shape();
     for (int i = 0; i < n && !rc; ++i) {
         cudaEventRecord(ev[3 * i], s->stream);
-        int e = launch_sweep(kMoveGrid, p.d_move, p.n_move, p.max_tile_beads, p.max_length, ms, s->stream);
+        int e = launch_sweep(kMoveGrid, p.d_move, p.n_move, p.max_tile_beads, p.max_length, ms, p.d_acc, s->stream);
         cudaEventRecord(ev[3 * i + 1], s->stream);
-        if (!e) e = launch_field(true, 0, p.d_field, p.n_field, fs, s->stream);
+        if (!e) e = launch_field(true, 0, p.d_field, p.n_field, fs, p.d_ef, s->stream);
+        if (!e)
+            e = launch_close(p.d_close, p.n_sys, p.d_acc, p.warps_per_tile(), p.d_ef, p.d_eb,
+                             kCloseMove | kCloseField | kCloseFlip | kCloseAdvance, s->stream);
         cudaEventRecord(ev[3 * i + 2], s->stream);
         if (e) rc = fail(SCMF_E_CUDA, "launch: %s", cudaGetErrorString((cudaError_t)e));
     }
@@ -448,8 +452,8 @@ scmf_status scmf_smc_move(scmf_system* s, int32_t n) {
     const LaunchShape sh = s->plan.move_shape();
     for (int i = 0; i < n; ++i) {
         CKL(launch_sweep(kMoveOnly, s->plan.d_move, s->plan.n_move, s->plan.max_tile_beads, s->plan.max_length, sh,
-                         s->stream));
-        CKL(launch_finalize_move(s->d_sys, s->stream));
+                         s->plan.d_acc, s->stream));
+        RET(s->plan.enqueue_close(kCloseMove | kCloseAdvance, s->stream));
     }
     CK(cudaStreamSynchronize(s->stream));
     return check_error_word(s);
@@ -520,7 +524,8 @@ scmf_status scmf_get_stats(const scmf_system* cs, scmf_stats* o) {
     SysDev d;
     RET(fetch_sysdev(s, &d));
     if (d.e_bond_step != d.step + 1u) {  // bond energy is computed on demand
-        CKL(launch_bond_energy(s->plan.d_move, s->plan.n_move, s->d_sys, s->plan.move_shape(), s->stream));
+        CKL(launch_bond_energy(s->plan.d_move, s->plan.n_move, s->plan.move_shape(), s->plan.d_eb, s->stream));
+        RET(s->plan.enqueue_close(kCloseBond, s->stream));
         RET(fetch_sysdev(s, &d));
     }
     std::memset(o, 0, sizeof *o);

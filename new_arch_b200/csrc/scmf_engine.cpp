@@ -241,13 +241,18 @@ scmf_tune resolve_tune(const scmf_tune* t) {
 void DevPlan::release() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graph_src) cudaGraphDestroy(graph_src);
-    if (d_move) cudaFree(d_move);
-    if (d_field) cudaFree(d_field);
+    void* ptrs[] = {d_move, d_field, d_close, d_acc, d_ef, d_eb};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
     graph = nullptr;
     graph_src = nullptr;
     d_move = nullptr;
     d_field = nullptr;
-    n_move = n_field = 0;
+    d_close = nullptr;
+    d_acc = nullptr;
+    d_ef = nullptr;
+    d_eb = nullptr;
+    n_move = n_field = n_sys = 0;
 }
 
 scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t) {
@@ -260,10 +265,18 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t) {
     n_types_uniform = p.n_types_uniform;
     max_chains = p.max_chains;
     linear = p.linear;
-    CK(cudaMalloc(&d_move, std::max<size_t>(1, p.move.size()) * sizeof(MoveTile)));
-    CK(cudaMalloc(&d_field, std::max<size_t>(1, p.field.size()) * sizeof(FieldTile)));
+    n_sys = (int)p.close.size();
+    const size_t nm = std::max<size_t>(1, p.move.size()), nf = std::max<size_t>(1, p.field.size());
+    CK(cudaMalloc(&d_move, nm * sizeof(MoveTile)));
+    CK(cudaMalloc(&d_field, nf * sizeof(FieldTile)));
+    CK(cudaMalloc(&d_close, std::max<size_t>(1, p.close.size()) * sizeof(SysClose)));
+    CK(cudaMalloc(&d_acc, nm * kMaxWarps * sizeof(unsigned)));
+    CK(cudaMalloc(&d_ef, nf * sizeof(double)));
+    CK(cudaMalloc(&d_eb, nm * sizeof(double)));
+    CK(cudaMemset(d_acc, 0, nm * kMaxWarps * sizeof(unsigned)));
     CK(cudaMemcpy(d_move, p.move.data(), p.move.size() * sizeof(MoveTile), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_field, p.field.data(), p.field.size() * sizeof(FieldTile), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_close, p.close.data(), p.close.size() * sizeof(SysClose), cudaMemcpyHostToDevice));
     return SCMF_OK;
 }
 
@@ -286,10 +299,15 @@ LaunchShape DevPlan::field_shape() const {
     return sh;
 }
 
-scmf_status DevPlan::enqueue_sweep(cudaStream_t st) const {
-    CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, move_shape(), st));
-    CKL(launch_field(true, 0, d_field, n_field, field_shape(), st));
+scmf_status DevPlan::enqueue_close(int mode, cudaStream_t st) const {
+    CKL(launch_close(d_close, n_sys, d_acc, warps_per_tile(), d_ef, d_eb, mode, st));
     return SCMF_OK;
+}
+
+scmf_status DevPlan::enqueue_sweep(cudaStream_t st) const {
+    CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, move_shape(), d_acc, st));
+    CKL(launch_field(true, 0, d_field, n_field, field_shape(), d_ef, st));
+    return enqueue_close(kCloseMove | kCloseField | kCloseFlip | kCloseAdvance, st);
 }
 
 scmf_status DevPlan::run_sweeps(cudaStream_t st, int n) {
@@ -332,6 +350,7 @@ using namespace scmf;
 scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
     const int64_t target_small = std::max<int64_t>(1, n_beads / (2 * 148));
     const size_t first_tile = p->move.size();
+    const size_t first_field = p->field.size();
     for (size_t a = 0; a < archs.size(); ++a) {
         const ArchHost& A = archs[a];
         if (A.n_chains == 0) continue;
@@ -371,6 +390,13 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
         ft.n_tiles_sys = ntile;
         p->field.push_back(ft);
     }
+    SysClose cl;
+    cl.sys = d_sys;
+    cl.move_first = (int32_t)first_tile;
+    cl.move_count = (int32_t)(p->move.size() - first_tile);
+    cl.field_first = (int32_t)first_field;
+    cl.field_count = (int32_t)(p->field.size() - first_field);
+    p->close.push_back(cl);
     if (p->n_types_uniform == 0 && p->field.size() == (size_t)ntile) p->n_types_uniform = spec.n_types;
     else if (p->n_types_uniform != spec.n_types) p->n_types_uniform = 0;
     // round the smem tile up so float4 staging stays aligned

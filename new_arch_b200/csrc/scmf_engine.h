@@ -52,6 +52,7 @@ void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d);
 struct Plan {
     std::vector<MoveTile> move;
     std::vector<FieldTile> field;
+    std::vector<SysClose> close;   // tile ranges of every system
     int max_tile_beads = 0;
     int max_length = 0;
     int n_types_uniform = 0;
@@ -63,7 +64,11 @@ struct Plan {
 struct DevPlan {
     MoveTile* d_move = nullptr;
     FieldTile* d_field = nullptr;
-    int n_move = 0, n_field = 0;
+    SysClose* d_close = nullptr;
+    unsigned* d_acc = nullptr;   // accept count per (move tile, warp)
+    double* d_ef = nullptr;      // field energy per field tile
+    double* d_eb = nullptr;      // bond energy per move tile
+    int n_move = 0, n_field = 0, n_sys = 0;
     int max_tile_beads = 0, max_length = 0, n_types_uniform = 0, max_chains = 0;
     bool linear = false;
     scmf_tune tune{};
@@ -73,8 +78,10 @@ struct DevPlan {
     scmf_status upload(const Plan& p, const scmf_tune& t);
     LaunchShape move_shape() const;
     LaunchShape field_shape() const;
-    // one fused sweep (move+grid, field) enqueued on `st`
+    int warps_per_tile() const { return tune.threads_move / 32; }
+    // one fused sweep (move+grid, field, close) enqueued on `st`
     scmf_status enqueue_sweep(cudaStream_t st) const;
+    scmf_status enqueue_close(int mode, cudaStream_t st) const;
     scmf_status run_sweeps(cudaStream_t st, int n);
 };
 

@@ -28,7 +28,8 @@ constexpr int kMaxDeg = 8;
 constexpr int kMaxColors = 8;
 constexpr int kMaxLength = 4096;    // beads per chain (16-bit neighbour indices)
 constexpr int kMaxTileBeads = 8192;  // beads staged in shared memory per tile
-constexpr int kSlots = 32;           // spread of the statistics atomics
+constexpr int kMaxWarps = 8;         // warps per move CTA (256 threads at most)
+constexpr int kSlots = 32;           // spread of the accept-count atomics
 constexpr uint32_t kInitStep = 0xFFFFFFFFu;
 
 // Per-bead architecture record.
@@ -47,6 +48,7 @@ struct ArchDev {
     int32_t color_off[kMaxColors + 1];
     uint32_t color_magic[kMaxColors];  // ceil(2^32 / n_in_colour): i / n == umulhi(i, magic)
     uint32_t len_magic;          // ceil(2^32 / length)
+    uint32_t tpc_magic;          // magic of ceil(length / 2): threads per chain in k_sweep_reg
     int32_t n_chains;
     int32_t chain_base;          // first global chain id of this architecture
     int64_t bead_base;           // first bead of this architecture in the system arrays
@@ -74,11 +76,9 @@ struct SysDev {
     // mutable state
     uint32_t step;        // completed sweeps
     uint32_t cur;         // counts[cur] holds the counts of the current positions
-    uint32_t field_done;  // field tiles finished in the current launch
     uint32_t error_word;
-    unsigned long long slot_acc[kSlots];
-    double slot_eb[kSlots];
-    double slot_ef[kSlots];
+    uint32_t pad0;
+    unsigned long long slot_acc[kSlots];  // accepted moves of the running sweep, cleared by k_close
     // statistics of the last completed sweep
     unsigned long long last_accepts, total_accepts, total_moves;
     double e_bond, e_field;
@@ -107,6 +107,16 @@ struct FieldTile {
 
 enum SweepMode : int { kMoveOnly = 0, kMoveGrid = 1, kGridOnly = 2 };
 
+// What k_close does for each system of a launch.
+enum CloseMode : int { kCloseMove = 1, kCloseField = 2, kCloseBond = 4, kCloseFlip = 8, kCloseAdvance = 16 };
+
+// The tile ranges of one system in a launch's work lists.
+struct SysClose {
+    SysDev* sys;
+    int32_t move_first, move_count;
+    int32_t field_first, field_count;
+};
+
 // Launchers (scmf_kernels.cu).  Every pointer is device memory.
 struct LaunchShape {
     int blocks;    // 0 = one CTA per tile
@@ -118,12 +128,16 @@ struct LaunchShape {
 };
 
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);
+// Move kernels add their accept counts into SysDev::slot_acc (32-way spread);
+// the field kernel writes one energy per tile into ef_part, the bond-energy
+// kernel one per move tile into eb_part; k_close sums and publishes them.
 int launch_sweep(int mode, const MoveTile* tiles, int n_tiles, int max_tile_beads, int max_length,
-                 LaunchShape shape, void* stream);
+                 LaunchShape shape, unsigned* acc_part, void* stream);
 int launch_field(bool fused, int force_update, const FieldTile* tiles, int n_tiles, LaunchShape shape,
-                 void* stream);
-int launch_finalize_move(SysDev* sys, void* stream);
-int launch_bond_energy(const MoveTile* tiles, int n_tiles, SysDev* sys, LaunchShape shape, void* stream);
+                 double* ef_part, void* stream);
+int launch_bond_energy(const MoveTile* tiles, int n_tiles, LaunchShape shape, double* eb_part, void* stream);
+int launch_close(const SysClose* list, int n_sys, const unsigned* acc_part, int warps_per_tile,
+                 const double* ef_part, const double* eb_part, int mode, void* stream);
 int launch_aos_to_soa(const float* aos, SysDev* sys, const ArchDev* arch, int n_arch, int64_t n_beads,
                       void* stream);
 int launch_soa_to_aos(float* aos, const SysDev* sys, const ArchDev* arch, int n_arch, int64_t n_beads,

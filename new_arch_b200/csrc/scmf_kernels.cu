@@ -154,7 +154,7 @@ size_t sweep_smem_bytes(int max_tile_beads, int max_length) {
 //   even beads colour 0, odd beads colour 1); neighbours are computed, not looked up.
 template <int MODE, bool LINEAR>
 __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ tiles, int n_tiles,
-                                                   int max_tile_beads, int max_length) {
+                                                   int max_tile_beads, int max_length, unsigned* __restrict__ acc_part) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sx = reinterpret_cast<float*>(smem_raw);
     float* sy = sx + max_tile_beads;
@@ -164,8 +164,6 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
     off = (off + (size_t)max_length * sizeof(BeadInfo) + 15) & ~(size_t)15;
     uint16_t* scol = reinterpret_cast<uint16_t*>(smem_raw + off);
     uint8_t* stype = reinterpret_cast<uint8_t*>(sinfo);  // LINEAR: types only
-    __shared__ unsigned s_acc[32];
-
     const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
         const MoveTile t = tiles[ti];
@@ -287,13 +285,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
                 __syncthreads();
             }
             nacc = warp_sum(nacc);
-            if (lane == 0) s_acc[warp] = nacc;
-            __syncthreads();
-            if (tid == 0) {
-                unsigned long long a = 0;
-                for (int w = 0; w < (T + 31) / 32; ++w) a += s_acc[w];
-                atomicAdd(&S->slot_acc[ti % kSlots], a);
-            }
+            if (lane == 0 && nacc) atomicAdd(&S->slot_acc[(ti * kMaxWarps + warp) % kSlots], (unsigned long long)nacc);
         }
 
         if (MODE == kGridOnly) {
@@ -346,7 +338,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
 #endif
 template <int MODE>
 __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(const MoveTile* __restrict__ tiles, int n_tiles,
-                                                          int warp_beads) {
+                                                          int warp_beads, unsigned* __restrict__ acc_part) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     float* sx = reinterpret_cast<float*>(smem_raw) + (size_t)warp * 3 * warp_beads;
@@ -361,7 +353,9 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
         const int cpw = (t.n_chains + nwarps - 1) / nwarps;
         const int c_begin = warp * cpw;
         const int nch = min(cpw, t.n_chains - c_begin);
-        if (nch <= 0) continue;
+        if (nch <= 0) {
+            continue;
+        }
         const int nb = nch * L;
         if (nb > warp_beads) {
             if (lane == 0) atomicOr(&S->error_word, 2u);
@@ -455,7 +449,7 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
                 __syncwarp();
             }
             nacc = warp_sum(nacc);
-            if (lane == 0 && nacc) atomicAdd(&S->slot_acc[(ti * nwarps + warp) % kSlots], (unsigned long long)nacc);
+            if (lane == 0 && nacc) atomicAdd(&S->slot_acc[(ti * kMaxWarps + warp) % kSlots], (unsigned long long)nacc);
         }
         if (MODE == kGridOnly) {
             for (int i = lane; i < nb; i += 32) {
@@ -482,10 +476,156 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
     }
 }
 
-// ------------------------------------------------------------------ field
-__device__ __forceinline__ double read_clear(double* p) {
-    return __longlong_as_double((long long)atomicExch(reinterpret_cast<unsigned long long*>(p), 0ull));
+// Linear chains of at most 64 beads, positions in registers.  Each thread owns
+// the bead pair (2t, 2t+1) of one chain (ceil(L/2) threads per chain, as many
+// chains per warp as fit).  Even half-sweep: bead 2t moves against 2t-1 (the
+// odd bead of lane-1, by shuffle) and 2t+1 (its own); odd half-sweep: bead
+// 2t+1 moves against 2t (its own, already moved) and 2t+2 (the even bead of
+// lane+1).  No shared memory, no block barrier; tiles are read and written
+// with coalesced float2 accesses.  Same trial and keys as k_sweep.
+#ifndef SCMF_REG_MIN_BLOCKS
+#define SCMF_REG_MIN_BLOCKS 3
+#endif
+template <int MODE>
+__global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const MoveTile* __restrict__ tiles, int n_tiles,
+                                                                        unsigned* __restrict__ acc_part) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
+        const MoveTile t = tiles[ti];
+        SysDev* S = t.sys;
+        const ArchDev* Ap = t.arch;
+        const int L = Ap->length;
+        const int tpc = (L + 1) >> 1;                        // threads per chain
+        const int cpw = 32 / tpc;                            // chains per warp
+        const int cs = (int)div_magic((uint32_t)lane, Ap->tpc_magic, tpc);
+        const int tt = lane - cs * tpc;                      // pair index in the chain
+        const int be = 2 * tt, bo = 2 * tt + 1;
+        MoveConsts c;
+        c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
+        c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
+        c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
+        const int64_t NC = S->n_cells;
+        uint32_t* cnt = S->counts[MODE == kMoveGrid ? (S->cur ^ 1u) : S->cur];
+        const bool c16 = S->count16 != 0;
+        const float* __restrict__ omega = S->omega;
+        const uint32_t step = S->step + 1u;
+        const uint32_t k0 = S->seed_lo, k1 = S->seed_hi;
+        const float cc1 = S->cdeg[1], ac41 = S->ac4deg[1], cc2 = S->cdeg[2], ac42 = S->ac4deg[2];
+        const int type_e = cs < cpw ? __ldg(Ap->types + min(be, L - 1)) : 0;
+        const int type_o = cs < cpw && bo < L ? __ldg(Ap->types + bo) : 0;
+        const bool pair_aligned = ((t.bead0 & 1) == 0) && ((L & 1) == 0);
+        unsigned nacc = 0;
+        for (int cbase = warp * cpw; cbase < t.n_chains; cbase += nwarps * cpw) {
+            const int chain = cbase + cs;
+            const bool live = cs < cpw && chain < t.n_chains;
+            const bool has_o = live && bo < L;
+            const int64_t g = t.bead0 + (int64_t)chain * L + be;
+            float xe = 0.0f, ye = 0.0f, ze = 0.0f, xo = 0.0f, yo = 0.0f, zo = 0.0f;
+            uint32_t gc = 0u;
+            if (live) {
+                if (pair_aligned) {
+                    const float2 vx = __ldcs(reinterpret_cast<const float2*>(S->x + g));
+                    const float2 vy = __ldcs(reinterpret_cast<const float2*>(S->y + g));
+                    const float2 vz = __ldcs(reinterpret_cast<const float2*>(S->z + g));
+                    xe = vx.x; xo = vx.y;
+                    ye = vy.x; yo = vy.y;
+                    ze = vz.x; zo = vz.y;
+                } else {
+                    xe = __ldcs(S->x + g);
+                    ye = __ldcs(S->y + g);
+                    ze = __ldcs(S->z + g);
+                    if (has_o) {
+                        xo = __ldcs(S->x + g + 1);
+                        yo = __ldcs(S->y + g + 1);
+                        zo = __ldcs(S->z + g + 1);
+                    }
+                }
+                gc = __ldg(S->chain_id + t.chain0 + chain);
+            }
+            if (MODE == kGridOnly) {
+                if (live) {
+                    const int64_t ie = (int64_t)type_e * NC + cell_of(c, xe, ye, ze);
+                    if (c16) atomicAdd(cnt + (ie >> 1), 1u << ((ie & 1) * 16)); else atomicAdd(cnt + ie, 1u);
+                }
+                if (has_o) {
+                    const int64_t io = (int64_t)type_o * NC + cell_of(c, xo, yo, zo);
+                    if (c16) atomicAdd(cnt + (io >> 1), 1u << ((io & 1) * 16)); else atomicAdd(cnt + io, 1u);
+                }
+                continue;
+            }
+            // even half-sweep
+            {
+                const float lx = __shfl_up_sync(0xffffffffu, xo, 1);
+                const float ly = __shfl_up_sync(0xffffffffu, yo, 1);
+                const float lz = __shfl_up_sync(0xffffffffu, zo, 1);
+                if (live) {
+                    float qx[2], qy[2], qz[2];
+                    int deg = 0;
+                    if (tt > 0) { qx[0] = lx; qy[0] = ly; qz[0] = lz; deg = 1; }
+                    if (has_o) { qx[deg] = xo; qy[deg] = yo; qz[deg] = zo; ++deg; }
+                    const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1);
+                    float px, py, pz;
+                    int cell;
+                    const bool acc = trial<2>(c, xe, ye, ze, qx, qy, qz, deg, deg == 2 ? cc2 : (deg == 1 ? cc1 : 0.0f),
+                                              deg == 2 ? ac42 : (deg == 1 ? ac41 : 0.0f), w,
+                                              omega + (int64_t)type_e * NC, px, py, pz, cell);
+                    if (acc) { xe = px; ye = py; ze = pz; }
+                    nacc += acc ? 1u : 0u;
+                    if (MODE == kMoveGrid) {
+                        const int64_t idx = (int64_t)type_e * NC + cell;
+                        if (c16) atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16)); else atomicAdd(cnt + idx, 1u);
+                    }
+                }
+            }
+            // odd half-sweep
+            {
+                const float rx = __shfl_down_sync(0xffffffffu, xe, 1);
+                const float ry = __shfl_down_sync(0xffffffffu, ye, 1);
+                const float rz = __shfl_down_sync(0xffffffffu, ze, 1);
+                if (has_o) {
+                    float qx[2], qy[2], qz[2];
+                    qx[0] = xe; qy[0] = ye; qz[0] = ze;
+                    int deg = 1;
+                    if (bo + 1 < L) { qx[1] = rx; qy[1] = ry; qz[1] = rz; deg = 2; }
+                    const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1);
+                    float px, py, pz;
+                    int cell;
+                    const bool acc = trial<2>(c, xo, yo, zo, qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
+                                              deg == 2 ? ac42 : ac41, w, omega + (int64_t)type_o * NC, px, py, pz,
+                                              cell);
+                    if (acc) { xo = px; yo = py; zo = pz; }
+                    nacc += acc ? 1u : 0u;
+                    if (MODE == kMoveGrid) {
+                        const int64_t idx = (int64_t)type_o * NC + cell;
+                        if (c16) atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16)); else atomicAdd(cnt + idx, 1u);
+                    }
+                }
+            }
+            if (live) {
+                if (pair_aligned) {
+                    __stcs(reinterpret_cast<float2*>(S->x + g), make_float2(xe, xo));
+                    __stcs(reinterpret_cast<float2*>(S->y + g), make_float2(ye, yo));
+                    __stcs(reinterpret_cast<float2*>(S->z + g), make_float2(ze, zo));
+                } else {
+                    __stcs(S->x + g, xe);
+                    __stcs(S->y + g, ye);
+                    __stcs(S->z + g, ze);
+                    if (has_o) {
+                        __stcs(S->x + g + 1, xo);
+                        __stcs(S->y + g + 1, yo);
+                        __stcs(S->z + g + 1, zo);
+                    }
+                }
+            }
+        }
+        if (MODE != kGridOnly) {
+            nacc = warp_sum(nacc);
+            if (lane == 0 && nacc) atomicAdd(&S->slot_acc[(ti * kMaxWarps + warp) % kSlots], (unsigned long long)nacc);
+        }
+    }
 }
+
+// ------------------------------------------------------------------ field
 
 // omega of one cell from its counts (NT = 0: runtime type count, up to
 // kMaxTypes).  Expression order matches the oracle's field_update():
@@ -602,10 +742,10 @@ __device__ __forceinline__ double field_cells4(int64_t cell, int64_t NC, float s
 }
 
 template <bool FUSED, int NT>
-__global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ tiles, int n_tiles, int force_update) {
+__global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ tiles, int n_tiles, int force_update,
+                                                double* __restrict__ ef_part) {
     __shared__ double s_ef[32];
     __shared__ float cf[kMaxTypes * kMaxTypes];
-    __shared__ int s_last;
     const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
         const FieldTile t = tiles[ti];
@@ -638,48 +778,68 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
         if (tid == 0) {
             double e = 0.0;
             for (int w = 0; w < (T + 31) / 32; ++w) e += s_ef[w];
-            atomicAdd(&S->slot_ef[ti % kSlots], e);
-            __threadfence();
-            const unsigned prev = atomicAdd(&S->field_done, 1u);
-            s_last = (prev == (unsigned)t.n_tiles_sys - 1u);
-        }
-        __syncthreads();
-        if (s_last && tid == 0) {
-            __threadfence();
-            double e_f = 0.0;
-            for (int s = 0; s < kSlots; ++s) e_f += read_clear(&S->slot_ef[s]);
-            S->e_field = e_f;
-            if (FUSED) {
-                unsigned long long a = 0;
-                for (int s = 0; s < kSlots; ++s) a += atomicExch(&S->slot_acc[s], 0ull);
-                S->last_accepts = a;
-                S->total_accepts += a;
-                S->total_moves += (unsigned long long)S->n_beads;
-                S->cur = cur ^ 1u;
-                S->step = sweep;
-            }
-            S->field_done = 0u;
-            __threadfence();
+            ef_part[ti] = e;
         }
         __syncthreads();
     }
 }
 
-__global__ void k_finalize_move(SysDev* S) {
-    if (threadIdx.x != 0) return;
-    unsigned long long a = 0;
-    for (int s = 0; s < kSlots; ++s) a += atomicExch(&S->slot_acc[s], 0ull);
-    S->last_accepts = a;
-    S->total_accepts += a;
-    S->total_moves += (unsigned long long)S->n_beads;
-    S->step = S->step + 1u;
+// Closes a launch for every system of the plan (one block per system): sums
+// the per-tile partials in a fixed order and updates the statistics, and for
+// a full sweep advances the step and makes the new counts current.
+__global__ void __launch_bounds__(256) k_close(const SysClose* __restrict__ list, int n_sys,
+                                                const unsigned* __restrict__ acc_part, int warps_per_tile,
+                                                const double* __restrict__ ef_part, const double* __restrict__ eb_part,
+                                                int mode) {
+    __shared__ unsigned long long s_a[256];
+    __shared__ double s_f[256];
+    const int tid = threadIdx.x, T = blockDim.x;
+    for (int si = blockIdx.x; si < n_sys; si += gridDim.x) {
+        const SysClose L = list[si];
+        SysDev* S = L.sys;
+        unsigned long long a = 0;
+        double f = 0.0;
+        if ((mode & kCloseMove) && tid < kSlots) {
+            a = S->slot_acc[tid];
+            S->slot_acc[tid] = 0ull;
+        }
+        if (mode & kCloseField)
+            for (int i = tid; i < L.field_count; i += T) f += ef_part[L.field_first + i];
+        if (mode & kCloseBond)
+            for (int i = tid; i < L.move_count; i += T) f += eb_part[L.move_first + i];
+        s_a[tid] = a;
+        s_f[tid] = f;
+        __syncthreads();
+        for (int o = T / 2; o > 0; o >>= 1) {
+            if (tid < o) {
+                s_a[tid] += s_a[tid + o];
+                s_f[tid] += s_f[tid + o];
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            if (mode & kCloseMove) {
+                S->last_accepts = s_a[0];
+                S->total_accepts += s_a[0];
+                S->total_moves += (unsigned long long)S->n_beads;
+            }
+            if (mode & kCloseField) S->e_field = s_f[0];
+            if (mode & kCloseBond) {
+                S->e_bond = s_f[0];
+                S->e_bond_step = S->step + 1u;
+            }
+            if (mode & kCloseFlip) S->cur ^= 1u;
+            if (mode & kCloseAdvance) S->step += 1u;
+        }
+        __syncthreads();
+    }
 }
 
 // Bond energy sum_bonds k |r_i - r_j|^2 of the current positions, each bond
-// once, accumulated into slot_eb; the last tile of the launch publishes it.
-__global__ void __launch_bounds__(256) k_bond_energy(const MoveTile* __restrict__ tiles, int n_tiles) {
+// once, one partial per tile (closed by k_close with kCloseBond).
+__global__ void __launch_bounds__(256) k_bond_energy(const MoveTile* __restrict__ tiles, int n_tiles,
+                                                      double* __restrict__ eb_part) {
     __shared__ double s_e[32];
-    __shared__ int s_last;
     const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
         const MoveTile t = tiles[ti];
@@ -710,19 +870,7 @@ __global__ void __launch_bounds__(256) k_bond_energy(const MoveTile* __restrict_
         if (tid == 0) {
             double a = 0.0;
             for (int w = 0; w < (T + 31) / 32; ++w) a += s_e[w];
-            atomicAdd(&S->slot_eb[ti % kSlots], a);
-            __threadfence();
-            s_last = (atomicAdd(&S->field_done, 1u) == (unsigned)t.n_tiles_sys - 1u);
-        }
-        __syncthreads();
-        if (s_last && tid == 0) {
-            __threadfence();
-            double a = 0.0;
-            for (int s = 0; s < kSlots; ++s) a += read_clear(&S->slot_eb[s]);
-            S->e_bond = a;
-            S->e_bond_step = S->step + 1u;
-            S->field_done = 0u;
-            __threadfence();
+            eb_part[ti] = a;
         }
         __syncthreads();
     }
@@ -833,64 +981,72 @@ int configure_kernels() {
 }
 
 template <int MODE>
-static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, LaunchShape sh, cudaStream_t st) {
+static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, LaunchShape sh, unsigned* acc,
+                          cudaStream_t st) {
     if (mtb > kMaxTileBeads || ml > kMaxLength || sh.threads > 256 || sh.threads < 32) return (int)cudaErrorInvalidValue;
     const int blocks = sh.blocks > 0 ? sh.blocks : n_tiles;
-    if (sh.linear) {
+    if (sh.linear && ml <= 64) {
+        k_sweep_reg<MODE><<<blocks, sh.threads, 0, st>>>(tiles, n_tiles, acc);
+    } else if (sh.linear) {
         // per-warp slice: ceil(chains per tile / warps) chains of the longest length
         const int nw = sh.threads / 32;
         const int wb = ((sh.max_chains + nw - 1) / nw) * ml;
         const size_t smem = (size_t)nw * 3 * wb * sizeof(float);
         if (smem > sweep_smem_bytes(kMaxTileBeads, kMaxLength)) return (int)cudaErrorInvalidValue;
-        k_sweep_linear<MODE><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, wb);
+        k_sweep_linear<MODE><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, wb, acc);
     } else {
         const size_t smem = sweep_smem_bytes(mtb, ml);
-        k_sweep<MODE, false><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml);
+        k_sweep<MODE, false><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml, acc);
     }
     return (int)cudaGetLastError();
 }
 
-int launch_sweep(int mode, const MoveTile* tiles, int n_tiles, int mtb, int ml, LaunchShape sh, void* stream) {
+int launch_sweep(int mode, const MoveTile* tiles, int n_tiles, int mtb, int ml, LaunchShape sh, unsigned* acc_part,
+                 void* stream) {
     if (n_tiles <= 0) return 0;
     cudaStream_t st = (cudaStream_t)stream;
-    if (mode == kMoveOnly) return launch_sweep_t<kMoveOnly>(tiles, n_tiles, mtb, ml, sh, st);
-    if (mode == kMoveGrid) return launch_sweep_t<kMoveGrid>(tiles, n_tiles, mtb, ml, sh, st);
-    return launch_sweep_t<kGridOnly>(tiles, n_tiles, mtb, ml, sh, st);
+    if (mode == kMoveOnly) return launch_sweep_t<kMoveOnly>(tiles, n_tiles, mtb, ml, sh, acc_part, st);
+    if (mode == kMoveGrid) return launch_sweep_t<kMoveGrid>(tiles, n_tiles, mtb, ml, sh, acc_part, st);
+    return launch_sweep_t<kGridOnly>(tiles, n_tiles, mtb, ml, sh, acc_part, st);
 }
 
 template <bool FUSED>
 static void launch_field_t(int nt, const FieldTile* tiles, int n_tiles, int force_update, int blocks, int threads,
-                           cudaStream_t st) {
+                           double* ef, cudaStream_t st) {
     if (nt == 2)
-        k_field<FUSED, 2><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update);
+        k_field<FUSED, 2><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef);
     else if (nt == 3)
-        k_field<FUSED, 3><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update);
+        k_field<FUSED, 3><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef);
     else if (nt == 1)
-        k_field<FUSED, 1><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update);
+        k_field<FUSED, 1><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef);
     else
-        k_field<FUSED, 0><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update);
+        k_field<FUSED, 0><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef);
 }
 
-int launch_field(bool fused, int force_update, const FieldTile* tiles, int n_tiles, LaunchShape sh, void* stream) {
+int launch_field(bool fused, int force_update, const FieldTile* tiles, int n_tiles, LaunchShape sh, double* ef_part,
+                 void* stream) {
     if (n_tiles <= 0) return 0;
     cudaStream_t st = (cudaStream_t)stream;
     const int blocks = sh.blocks > 0 ? sh.blocks : n_tiles;
     const int threads = sh.threads > 256 ? 256 : sh.threads;
     if (fused)
-        launch_field_t<true>(sh.n_types, tiles, n_tiles, force_update, blocks, threads, st);
+        launch_field_t<true>(sh.n_types, tiles, n_tiles, force_update, blocks, threads, ef_part, st);
     else
-        launch_field_t<false>(sh.n_types, tiles, n_tiles, force_update, blocks, threads, st);
+        launch_field_t<false>(sh.n_types, tiles, n_tiles, force_update, blocks, threads, ef_part, st);
     return (int)cudaGetLastError();
 }
 
-int launch_bond_energy(const MoveTile* tiles, int n_tiles, SysDev*, LaunchShape sh, void* stream) {
+int launch_bond_energy(const MoveTile* tiles, int n_tiles, LaunchShape sh, double* eb_part, void* stream) {
     if (n_tiles <= 0) return 0;
-    k_bond_energy<<<n_tiles, sh.threads > 256 ? 256 : sh.threads, 0, (cudaStream_t)stream>>>(tiles, n_tiles);
+    k_bond_energy<<<n_tiles, sh.threads > 256 ? 256 : sh.threads, 0, (cudaStream_t)stream>>>(tiles, n_tiles, eb_part);
     return (int)cudaGetLastError();
 }
 
-int launch_finalize_move(SysDev* sys, void* stream) {
-    k_finalize_move<<<1, 32, 0, (cudaStream_t)stream>>>(sys);
+int launch_close(const SysClose* list, int n_sys, const unsigned* acc_part, int warps_per_tile, const double* ef_part,
+                 const double* eb_part, int mode, void* stream) {
+    if (n_sys <= 0) return 0;
+    k_close<<<n_sys < 1024 ? n_sys : 1024, 256, 0, (cudaStream_t)stream>>>(list, n_sys, acc_part, warps_per_tile,
+                                                                             ef_part, eb_part, mode);
     return (int)cudaGetLastError();
 }
 
