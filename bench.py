@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--forms", choices=["all", "plain"], default="all")
+    ap.add_argument("--forms", choices=["all", "plain", "batched", "served"], default="all")
     ap.add_argument("--batched-sweeps", type=int, default=100)
     ap.add_argument("--served-requests", type=int, default=2000)
     ap.add_argument("--served-rate", type=float, default=200.0)
@@ -274,9 +274,10 @@ def run_ours(args):
             "phases": {"move_grid_ms": ms_move / args.steps, "field_ms": ms_field / args.steps,
                        "field_gbs": field_gbs, "field_frac": field_gbs / peak}}
 
-    # ---- batched vs plain on the same 256-system mix (rank-local)
-    if args.forms == "all":
+    # ---- batched vs plain on the same 256-system mix, and the served stream (rank-local)
+    if args.forms in ("all", "batched"):
         line["batched"] = run_batched(nb, batched_mix, args, torch)
+    if args.forms in ("all", "served"):
         line["served"] = run_served(nb, served_request, args)
 
     # ---- CPU oracle on this host (rank 0, N=1 only)

@@ -32,15 +32,10 @@ namespace {
 size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 template <typename T>
-scmf_status dalloc(T** p, size_t bytes, size_t* total) {
+scmf_status dalloc(T** p, size_t bytes, size_t* total, cudaStream_t st) {
     bytes = round_up(std::max<size_t>(bytes, 16), 256);
-    cudaError_t e = cudaMalloc((void**)p, bytes);
-    if (e != cudaSuccess) {
-        *p = nullptr;
-        cudaGetLastError();
-        return fail(e == cudaErrorMemoryAllocation ? SCMF_E_NOMEM : SCMF_E_CUDA, "cudaMalloc(%zu): %s", bytes,
-                    cudaGetErrorString(e));
-    }
+    scmf_status rc = dev_alloc((void**)p, bytes, st);
+    if (rc) return rc;
     *total += bytes;
     return SCMF_OK;
 }
@@ -50,9 +45,11 @@ void free_system(scmf_system* s) {
     s->plan.release();
     void* ptrs[] = {s->x, s->y, s->z, s->chain_id, s->counts[0], s->counts[1], s->omega, s->d_sys, s->d_arch,
                     s->d_arch_blob, s->d_aos, s->d_u32};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
-    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    for (void* p : ptrs) dev_free(p, s->stream);
+    if (s->own_stream && s->stream) {
+        cudaStreamSynchronize(s->stream);
+        cudaStreamDestroy(s->stream);
+    }
     delete s;
 }
 
@@ -84,7 +81,7 @@ scmf_status field_now(scmf_system* s) {
 scmf_status ensure_aos(scmf_system* s) {
     if (s->d_aos) return SCMF_OK;
     size_t dummy = 0;
-    return dalloc(&s->d_aos, (size_t)s->n_beads * 3 * sizeof(float), &dummy);
+    return dalloc(&s->d_aos, (size_t)s->n_beads * 3 * sizeof(float), &dummy, s->stream);
 }
 
 scmf_status check_error_word(const scmf_system* s) {
@@ -274,17 +271,19 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
     size_t tot = 0;
     const size_t nbp = (size_t)((s->n_beads + 3) & ~(int64_t)3);
     const size_t cells_t = (size_t)s->n_cells * spec->n_types;
-    if ((rc = dalloc(&s->x, nbp * 4, &tot)) || (rc = dalloc(&s->y, nbp * 4, &tot)) || (rc = dalloc(&s->z, nbp * 4, &tot)) ||
-        (rc = dalloc(&s->chain_id, (size_t)s->n_chains * 4, &tot)) ||
-        (rc = dalloc(&s->counts[0], counts_bytes(s), &tot)) || (rc = dalloc(&s->counts[1], counts_bytes(s), &tot)) ||
-        (rc = dalloc(&s->omega, cells_t * 4, &tot)) || (rc = dalloc(&s->d_sys, sizeof(SysDev), &tot)) ||
-        (rc = dalloc(&s->d_arch, s->archs.size() * sizeof(ArchDev), &tot)))
+    cudaStream_t st = s->stream;
+    if ((rc = dalloc(&s->x, nbp * 4, &tot, st)) || (rc = dalloc(&s->y, nbp * 4, &tot, st)) ||
+        (rc = dalloc(&s->z, nbp * 4, &tot, st)) || (rc = dalloc(&s->chain_id, (size_t)s->n_chains * 4, &tot, st)) ||
+        (rc = dalloc(&s->counts[0], counts_bytes(s), &tot, st)) ||
+        (rc = dalloc(&s->counts[1], counts_bytes(s), &tot, st)) || (rc = dalloc(&s->omega, cells_t * 4, &tot, st)) ||
+        (rc = dalloc(&s->d_sys, sizeof(SysDev), &tot, st)) ||
+        (rc = dalloc(&s->d_arch, s->archs.size() * sizeof(ArchDev), &tot, st)))
         return bail(rc);
     // architecture tables
     size_t blob = 0;
     auto arch_bytes = [](int L) { return round_up((size_t)L * (sizeof(BeadInfo) + sizeof(uint16_t) + 1) + 16, 256); };
     for (const auto& a : s->archs) blob += arch_bytes(a.length);
-    if ((rc = dalloc(&s->d_arch_blob, blob, &tot))) return bail(rc);
+    if ((rc = dalloc(&s->d_arch_blob, blob, &tot, st))) return bail(rc);
     s->device_bytes = tot;
     std::vector<char> hblob(blob, 0);
     size_t off = 0;
@@ -314,8 +313,9 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
         d.init_sigma = a.init_sigma;
         s->h_arch.push_back(d);
     }
-    if (cudaMemcpy(s->d_arch_blob, hblob.data(), blob, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(s->d_arch, s->h_arch.data(), s->h_arch.size() * sizeof(ArchDev), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpyAsync(s->d_arch_blob, hblob.data(), blob, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(s->d_arch, s->h_arch.data(), s->h_arch.size() * sizeof(ArchDev), cudaMemcpyHostToDevice, st) !=
+            cudaSuccess)
         return bail(fail(SCMF_E_CUDA, "upload of architecture tables failed"));
     std::vector<uint32_t> ids(s->n_chains);
     std::iota(ids.begin(), ids.end(), 0u);
@@ -326,15 +326,18 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
     h.counts[0] = s->counts[0];
     h.counts[1] = s->counts[1];
     h.omega = s->omega;
-    if (cudaMemcpy(s->chain_id, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(s->d_sys, &h, sizeof h, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(s->x, 0, nbp * 4) != cudaSuccess || cudaMemset(s->y, 0, nbp * 4) != cudaSuccess ||
-        cudaMemset(s->z, 0, nbp * 4) != cudaSuccess || cudaMemset(s->counts[0], 0, counts_bytes(s)) != cudaSuccess ||
-        cudaMemset(s->counts[1], 0, counts_bytes(s)) != cudaSuccess || cudaMemset(s->omega, 0, cells_t * 4) != cudaSuccess)
+    if (cudaMemcpyAsync(s->chain_id, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(s->d_sys, &h, sizeof h, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemsetAsync(s->x, 0, nbp * 4, st) != cudaSuccess || cudaMemsetAsync(s->y, 0, nbp * 4, st) != cudaSuccess ||
+        cudaMemsetAsync(s->z, 0, nbp * 4, st) != cudaSuccess ||
+        cudaMemsetAsync(s->counts[0], 0, counts_bytes(s), st) != cudaSuccess ||
+        cudaMemsetAsync(s->counts[1], 0, counts_bytes(s), st) != cudaSuccess ||
+        cudaMemsetAsync(s->omega, 0, cells_t * 4, st) != cudaSuccess)
         return bail(fail(SCMF_E_CUDA, "initialisation of device buffers failed"));
     Plan p;
     const scmf_tune t = default_tune();
-    if ((rc = s->append_plan(t, &p)) || (rc = s->plan.upload(p, t))) return bail(rc);
+    // upload() waits for the stream, so the host staging above may go out of scope
+    if ((rc = s->append_plan(t, &p)) || (rc = s->plan.upload(p, t, st))) return bail(rc);
     *out = s;
     return SCMF_OK;
 }
@@ -489,7 +492,7 @@ scmf_status scmf_get_counts(const scmf_system* cs, uint32_t* out, size_t n) {
     if (s->spec.p.count_bits == 16) {
         if (!s->d_u32) {
             size_t dummy = 0;
-            RET(dalloc(&s->d_u32, want * 4, &dummy));
+            RET(dalloc(&s->d_u32, want * 4, &dummy, s->stream));
         }
         CKL(launch_unpack_counts16(s->d_sys, s->d_u32, (int64_t)want, s->stream));
         CK(cudaMemcpyAsync(out, s->d_u32, want * 4, cudaMemcpyDeviceToHost, s->stream));
@@ -569,7 +572,7 @@ scmf_status scmf_batch_create(scmf_system* const* systems, int32_t n, const scmf
     const scmf_tune t = resolve_tune(tune);
     Plan p;
     for (auto* s : b->systems) s->append_plan(t, &p);
-    scmf_status rc = b->plan.upload(p, t);
+    scmf_status rc = b->plan.upload(p, t, b->stream);
     if (rc) {
         scmf_batch_destroy(b);
         return rc;
@@ -630,9 +633,9 @@ struct Snapshot {
 static scmf_status snap_take(scmf_system* s, Snapshot* sn, cudaStream_t st) {
     const size_t nb = (size_t)s->n_beads * 4, cb = counts_bytes(s), ob = (size_t)s->n_cells * s->spec.n_types * 4;
     size_t dummy = 0;
-    RET(dalloc(&sn->xyz, 3 * nb, &dummy));
-    RET(dalloc(&sn->cnt, 2 * cb, &dummy));
-    RET(dalloc(&sn->om, ob, &dummy));
+    RET(dalloc(&sn->xyz, 3 * nb, &dummy, st));
+    RET(dalloc(&sn->cnt, 2 * cb, &dummy, st));
+    RET(dalloc(&sn->om, ob, &dummy, st));
     CK(cudaMemcpyAsync(sn->xyz, s->x, nb, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync((char*)sn->xyz + nb, s->y, nb, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync((char*)sn->xyz + 2 * nb, s->z, nb, cudaMemcpyDeviceToDevice, st));
@@ -656,10 +659,10 @@ static scmf_status snap_restore(scmf_system* s, Snapshot* sn, cudaStream_t st) {
     return SCMF_OK;
 }
 
-static void snap_free(Snapshot* sn) {
-    if (sn->xyz) cudaFree(sn->xyz);
-    if (sn->cnt) cudaFree(sn->cnt);
-    if (sn->om) cudaFree(sn->om);
+static void snap_free(Snapshot* sn, cudaStream_t st) {
+    dev_free(sn->xyz, st);
+    dev_free(sn->cnt, st);
+    dev_free(sn->om, st);
     sn->xyz = nullptr;
     sn->cnt = nullptr;
     sn->om = nullptr;
@@ -685,7 +688,7 @@ scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps, scmf_tune* out) {
         DevPlan dp;
         Plan p;
         for (auto* s : b->systems) s->append_plan(t, &p);
-        RET(dp.upload(p, t));
+        RET(dp.upload(p, t, b->stream));
         scmf_status r = dp.run_sweeps(b->stream, 1);  // warm-up (and graph capture)
         if (!r) {
             cudaEventRecord(e0, b->stream);
@@ -733,13 +736,13 @@ scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps, scmf_tune* out) {
             }
         }
     }
-    for (auto& sn : snaps) snap_free(&sn);
+    for (auto& sn : snaps) snap_free(&sn, b->stream);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
     Plan p;
     for (auto* s : b->systems) s->append_plan(best, &p);
-    RET(b->plan.upload(p, best));
+    RET(b->plan.upload(p, best, b->stream));
     if (out) *out = best;
     return SCMF_OK;
 }

@@ -47,6 +47,32 @@ const char* last_error_cstr() { return g_last_error.c_str(); }
             return fail(SCMF_E_CUDA, "%s: %s", #expr, cudaGetErrorString((cudaError_t)e_));          \
     } while (0)
 
+scmf_status dev_alloc(void** p, size_t bytes, cudaStream_t st) {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    });
+    bytes = (std::max<size_t>(bytes, 16) + 255) / 256 * 256;
+    cudaError_t e = cudaMallocAsync(p, bytes, st);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? SCMF_E_NOMEM : SCMF_E_CUDA, "cudaMallocAsync(%zu): %s", bytes,
+                    cudaGetErrorString(e));
+    }
+    return SCMF_OK;
+}
+
+void dev_free(void* p, cudaStream_t st) {
+    if (p) cudaFreeAsync(p, st);
+}
+
 // ceil(2^32 / n): for i * n < 2^32, i / n == umulhi(i, magic).  n == 1 has no
 // 32-bit magic; the kernels test for it.
 uint32_t magic_for(uint32_t n) {
@@ -242,8 +268,7 @@ void DevPlan::release() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graph_src) cudaGraphDestroy(graph_src);
     void* ptrs[] = {d_move, d_field, d_close, d_acc, d_ef, d_eb};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    for (void* p : ptrs) dev_free(p, stream);
     graph = nullptr;
     graph_src = nullptr;
     d_move = nullptr;
@@ -255,8 +280,9 @@ void DevPlan::release() {
     n_move = n_field = n_sys = 0;
 }
 
-scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t) {
+scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t, cudaStream_t st) {
     release();
+    stream = st;
     tune = t;
     n_move = (int)p.move.size();
     n_field = (int)p.field.size();
@@ -267,16 +293,19 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t) {
     linear = p.linear;
     n_sys = (int)p.close.size();
     const size_t nm = std::max<size_t>(1, p.move.size()), nf = std::max<size_t>(1, p.field.size());
-    CK(cudaMalloc(&d_move, nm * sizeof(MoveTile)));
-    CK(cudaMalloc(&d_field, nf * sizeof(FieldTile)));
-    CK(cudaMalloc(&d_close, std::max<size_t>(1, p.close.size()) * sizeof(SysClose)));
-    CK(cudaMalloc(&d_acc, nm * kMaxWarps * sizeof(unsigned)));
-    CK(cudaMalloc(&d_ef, nf * sizeof(double)));
-    CK(cudaMalloc(&d_eb, nm * sizeof(double)));
-    CK(cudaMemset(d_acc, 0, nm * kMaxWarps * sizeof(unsigned)));
-    CK(cudaMemcpy(d_move, p.move.data(), p.move.size() * sizeof(MoveTile), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_field, p.field.data(), p.field.size() * sizeof(FieldTile), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(d_close, p.close.data(), p.close.size() * sizeof(SysClose), cudaMemcpyHostToDevice));
+    scmf_status rc;
+    if ((rc = dev_alloc((void**)&d_move, nm * sizeof(MoveTile), st)) ||
+        (rc = dev_alloc((void**)&d_field, nf * sizeof(FieldTile), st)) ||
+        (rc = dev_alloc((void**)&d_close, std::max<size_t>(1, p.close.size()) * sizeof(SysClose), st)) ||
+        (rc = dev_alloc((void**)&d_acc, nm * kMaxWarps * sizeof(unsigned), st)) ||
+        (rc = dev_alloc((void**)&d_ef, nf * sizeof(double), st)) || (rc = dev_alloc((void**)&d_eb, nm * sizeof(double), st)))
+        return rc;
+    CK(cudaMemsetAsync(d_acc, 0, nm * kMaxWarps * sizeof(unsigned), st));
+    CK(cudaMemcpyAsync(d_move, p.move.data(), p.move.size() * sizeof(MoveTile), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_field, p.field.data(), p.field.size() * sizeof(FieldTile), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d_close, p.close.data(), p.close.size() * sizeof(SysClose), cudaMemcpyHostToDevice, st));
+    // the host vectors may go away after return: wait for the (pageable) copies
+    CK(cudaStreamSynchronize(st));
     return SCMF_OK;
 }
 
@@ -337,8 +366,8 @@ scmf_status DevPlan::run_sweeps(cudaStream_t st, int n) {
 }
 
 scmf_status fetch_sysdev(const scmf_system* s, SysDev* out) {
+    CK(cudaMemcpyAsync(out, s->d_sys, sizeof(SysDev), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
-    CK(cudaMemcpy(out, s->d_sys, sizeof(SysDev), cudaMemcpyDeviceToHost));
     return SCMF_OK;
 }
 

@@ -42,6 +42,12 @@ struct ArchHost {
     int color_off[kMaxColors + 1] = {};
 };
 
+// Stream-ordered device memory (cudaMallocAsync / cudaFreeAsync on the
+// device's default pool, kept cached): creating and destroying systems and
+// plans never synchronises the device.
+scmf_status dev_alloc(void** p, size_t bytes, cudaStream_t st);
+void dev_free(void* p, cudaStream_t st);
+
 scmf_status validate_spec(const scmf_spec& s);
 scmf_status prepare_archs(const scmf_spec& s, std::vector<ArchHost>* out, int64_t* n_beads, int* n_chains);
 uint32_t magic_for(uint32_t n);
@@ -74,8 +80,9 @@ struct DevPlan {
     scmf_tune tune{};
     cudaGraphExec_t graph = nullptr;
     cudaGraph_t graph_src = nullptr;
+    cudaStream_t stream = nullptr;  // allocations of the plan are ordered on it
     void release();
-    scmf_status upload(const Plan& p, const scmf_tune& t);
+    scmf_status upload(const Plan& p, const scmf_tune& t, cudaStream_t st);
     LaunchShape move_shape() const;
     LaunchShape field_shape() const;
     int warps_per_tile() const { return tune.threads_move / 32; }

@@ -141,7 +141,7 @@ void scmf_server::run() {
         if (!plan_valid) {
             Plan p;
             for (auto& a : active) a.sys->append_plan(tune, &p);
-            scmf_status rc = plan.upload(p, tune);
+            scmf_status rc = plan.upload(p, tune, stream);
             if (rc) {
                 for (auto& a : active) finish(this, a, rc);
                 active.clear();

@@ -13,7 +13,7 @@ from .spec import SystemSpec
 
 
 class Server:
-    def __init__(self, hbm_budget_bytes: int, max_active: int = 0, sweeps_per_round: int = 0, use_graph: bool = True):
+    def __init__(self, hbm_budget_bytes: int, max_active: int = 0, sweeps_per_round: int = 0, use_graph: bool = False):
         opts = _lib.ServerOpts(int(hbm_budget_bytes), int(max_active), int(sweeps_per_round), int(bool(use_graph)), 0)
         self._h = C.c_void_p()
         check(lib().scmf_server_create(C.byref(opts), C.byref(self._h)))
