@@ -166,6 +166,10 @@ scmf_status scmf_get_counts(const scmf_system* sys, uint32_t* out, size_t n);
 scmf_status scmf_get_omega(const scmf_system* sys, float* out, size_t n);
 scmf_status scmf_set_omega(scmf_system* sys, const float* in, size_t n);
 scmf_status scmf_get_stats(const scmf_system* sys, scmf_stats* out);
+/* The statistics a sweep produces by itself (step, accepts, field energy) in
+ * one small device-to-host read; e_bond is NaN unless it is current (it is
+ * computed on demand by scmf_get_stats). */
+scmf_status scmf_get_sweep_stats(const scmf_system* sys, scmf_stats* out);
 
 /* Diagnostics: evaluates the device arithmetic (Philox4x32-10 with counter
  * (c0,c1,c2,c3) = (i, 0, 0, 0) and the given key, then log(u01(w.x)),

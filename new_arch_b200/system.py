@@ -105,6 +105,13 @@ class System:
         check(lib().scmf_get_stats(self._h, C.byref(st)))
         return {k: getattr(st, k) for k, _ in _lib.Stats._fields_ if k != "reserved"}
 
+    def sweep_stats(self) -> dict:
+        """Step, accepts and field energy of the last sweep (one small read; no
+        bond-energy pass, e_bond is NaN unless current)."""
+        st = _lib.Stats()
+        check(lib().scmf_get_sweep_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _lib.Stats._fields_ if k != "reserved"}
+
     # ----------------------------------------------------------------- steps
     def step(self, n_sweeps: int = 1) -> None:
         check(lib().scmf_step(self._h, int(n_sweeps)))

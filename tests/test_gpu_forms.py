@@ -165,6 +165,14 @@ def test_full_size_properties(nb, which):
         st = s.stats()
     assert int(cnt.sum()) == spec.n_beads
     assert st["step"] == 4 and st["total_moves"] == 4 * spec.n_beads
+    # the cheap per-sweep read agrees on everything the sweep itself produced
+    with nb.System(spec) as s2:
+        s2.init_coords()
+        s2.step(2)
+        a, b = s2.sweep_stats(), s2.stats()
+        assert a["step"] == b["step"] == 2 and a["total_accepts"] == b["total_accepts"]
+        assert a["e_field"] == b["e_field"] and np.isnan(a["e_bond"]) and b["e_bond"] > 0
+        assert s2.sweep_stats()["e_bond"] == b["e_bond"]
     set_threads(os.cpu_count() or 1)
     o = OracleSystem(spec)
     o.set_coords(xyz)
