@@ -74,14 +74,24 @@ __global__ void k_init_coords(SysDev* __restrict__ S, const ArchDev* __restrict_
 struct MoveConsts {
     float k, k2, A, R, inv_dx, inv_dy, inv_dz;
     int nx, ny, nz;
+    bool pow2;  // nx, ny, nz all powers of two
 };
 
 __device__ __forceinline__ int cell_of(const MoveConsts& c, float x, float y, float z) {
-    const int ix = fold(x, c.inv_dx, c.nx);
-    const int iy = fold(y, c.inv_dy, c.ny);
-    const int iz = fold(z, c.inv_dz, c.nz);
+    int ix, iy, iz;
+    if (c.pow2) {
+        ix = fold_pow2(x, c.inv_dx, c.nx - 1);
+        iy = fold_pow2(y, c.inv_dy, c.ny - 1);
+        iz = fold_pow2(z, c.inv_dz, c.nz - 1);
+    } else {
+        ix = fold(x, c.inv_dx, c.nx);
+        iy = fold(y, c.inv_dy, c.ny);
+        iz = fold(z, c.inv_dz, c.nz);
+    }
     return ix + c.nx * (iy + c.ny * iz);
 }
+
+__device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
 
 // One smart-MC trial (device_function.cu:637-717, 562-588, 444-454) of a bead
 // at (x,y,z) with deg bonded neighbours q[0..deg) in ascending bead order.
@@ -179,6 +189,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
         c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
         c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
         c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
+        c.pow2 = is_pow2(c.nx) && is_pow2(c.ny) && is_pow2(c.nz);
         const uint32_t len_magic = Ap->len_magic;
         for (int i = tid; i < L; i += T) {
             if (LINEAR) {
@@ -365,6 +376,7 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
         c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
         c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
         c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
+        c.pow2 = is_pow2(c.nx) && is_pow2(c.ny) && is_pow2(c.nz);
         const uint32_t len_magic = Ap->len_magic;
         const int64_t g0 = t.bead0 + (int64_t)c_begin * L;
         float* gx = S->x + g0;
@@ -504,6 +516,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
         c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
         c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
         c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
+        c.pow2 = is_pow2(c.nx) && is_pow2(c.ny) && is_pow2(c.nz);
         const int64_t NC = S->n_cells;
         uint32_t* cnt = S->counts[MODE == kMoveGrid ? (S->cur ^ 1u) : S->cur];
         const bool c16 = S->count16 != 0;

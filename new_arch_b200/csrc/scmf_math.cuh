@@ -132,4 +132,11 @@ __device__ __forceinline__ int fold(float x, float inv_d, int n) {
     return i;
 }
 
+// The same fold for a power-of-two n: the low log2(n) bits of the mantissa
+// of t + 1.5*2^23 (rounded down) are floor(t) mod n, because 0x4B400000, the
+// offset of that mantissa, has no bits below 2^22.  Exact for |t| < 2^22.
+__device__ __forceinline__ int fold_pow2(float x, float inv_d, int mask) {
+    return __float_as_int(__fadd_rd(__fmul_rn(x, inv_d), 0x1.8p23f)) & mask;
+}
+
 }  // namespace scmf
