@@ -103,8 +103,9 @@ __device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
 // final cell index.
 template <int MAXDEG>
 __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, float z, const float* qx,
-                                      const float* qy, const float* qz, int deg, float cc, float ac4, uint4 w,
-                                      const float* __restrict__ w_t, float& px, float& py, float& pz, int& cell) {
+                                      const float* qy, const float* qz, int deg, float cc, float ac4, float n0,
+                                      float n1, float n2, uint32_t aw, const float* __restrict__ w_t, float& px,
+                                      float& py, float& pz, int& cell) {
     const float k2 = c.k2, A = c.A, R = c.R;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
 #pragma unroll
@@ -115,8 +116,6 @@ __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, flo
             fz = __fmaf_rn(__fsub_rn(qz[d], z), k2, fz);
         }
     }
-    float n0, n1, n2;
-    normals3(w, n0, n1, n2);
     const float dx = __fmaf_rn(A, fx, __fmul_rn(R, n0));
     const float dy = __fmaf_rn(A, fy, __fmul_rn(R, n1));
     const float dz = __fmaf_rn(A, fz, __fmul_rn(R, n2));
@@ -134,11 +133,25 @@ __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, flo
     if (dE < 0.0f)
         acc = true;
     else if (dE < 17.0f)
-        acc = log_f(u01(accept_word(w))) < -dE;
+        acc = log_f(u01(aw)) < -dE;
     else
         acc = false;
     cell = acc ? c_new : c_old;
     return acc;
+}
+
+// Philox block and normals of bead b of chain gc (odd beads also draw the
+// block of b-1 for its spare sine).
+__device__ __forceinline__ uint32_t bead_normals(uint32_t gc, int b, uint32_t step, uint32_t k0, uint32_t k1,
+                                                 float& n0, float& n1, float& n2) {
+    const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1);
+    if (b & 1) {
+        const float sp = spare_of(philox4x32_10(make_uint4(gc, (uint32_t)(b - 1), step, 0u), k0, k1));
+        normals3_odd(sp, w, n0, n1, n2);
+    } else {
+        normals3(w, n0, n1, n2);
+    }
+    return accept_word(w);
 }
 
 template <typename T>
@@ -272,12 +285,13 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
                             }
                         }
                     }
-                    const uint4 w = philox4x32_10(make_uint4(__ldg(cid + cl), (uint32_t)b, step, 0u), k0, k1);
+                    float n0, n1, n2;
+                    const uint32_t aw = bead_normals(__ldg(cid + cl), b, step, k0, k1, n0, n1, n2);
                     float px, py, pz;
                     int cell;
                     const bool acc = trial<LINEAR ? 2 : kMaxDeg>(c, sx[base + b], sy[base + b], sz[base + b], qx, qy,
                                                                  qz, deg, deg == 2 ? cc2 : S->cdeg[deg],
-                                                                 deg == 2 ? ac42 : S->ac4deg[deg], w,
+                                                                 deg == 2 ? ac42 : S->ac4deg[deg], n0, n1, n2, aw,
                                                                  omega + (int64_t)type * NC, px, py, pz, cell);
                     if (acc) {
                         sx[base + b] = px;
@@ -438,12 +452,13 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
                         ++deg;
                     }
                     const int type = __ldg(types + b);
-                    const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1);
+                    float n0, n1, n2;
+                    const uint32_t aw = bead_normals(gc, b, step, k0, k1, n0, n1, n2);
                     float px, py, pz;
                     int cell;
                     const bool acc = trial<2>(c, sx[me], sy[me], sz[me], qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
-                                              deg == 2 ? ac42 : ac41, w, omega + (int64_t)type * NC, px, py, pz,
-                                              cell);
+                                              deg == 2 ? ac42 : ac41, n0, n1, n2, aw, omega + (int64_t)type * NC, px,
+                                              py, pz, cell);
                     if (acc) {
                         sx[me] = px;
                         sy[me] = py;
@@ -566,6 +581,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                 }
                 continue;
             }
+            float spare = 0.0f;  // spare sine of the even bead's block, first normal of the odd bead
             // even half-sweep
             {
                 const float lx = __shfl_up_sync(0xffffffffu, xo, 1);
@@ -577,10 +593,12 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     if (tt > 0) { qx[0] = lx; qy[0] = ly; qz[0] = lz; deg = 1; }
                     if (has_o) { qx[deg] = xo; qy[deg] = yo; qz[deg] = zo; ++deg; }
                     const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1);
+                    float n0, n1, n2;
+                    normals3_spare(w, n0, n1, n2, spare);
                     float px, py, pz;
                     int cell;
                     const bool acc = trial<2>(c, xe, ye, ze, qx, qy, qz, deg, deg == 2 ? cc2 : (deg == 1 ? cc1 : 0.0f),
-                                              deg == 2 ? ac42 : (deg == 1 ? ac41 : 0.0f), w,
+                                              deg == 2 ? ac42 : (deg == 1 ? ac41 : 0.0f), n0, n1, n2, accept_word(w),
                                               omega + (int64_t)type_e * NC, px, py, pz, cell);
                     if (acc) { xe = px; ye = py; ze = pz; }
                     nacc += acc ? 1u : 0u;
@@ -601,11 +619,13 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     int deg = 1;
                     if (bo + 1 < L) { qx[1] = rx; qy[1] = ry; qz[1] = rz; deg = 2; }
                     const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1);
+                    float n0, n1, n2;
+                    normals3_odd(spare, w, n0, n1, n2);
                     float px, py, pz;
                     int cell;
                     const bool acc = trial<2>(c, xo, yo, zo, qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
-                                              deg == 2 ? ac42 : ac41, w, omega + (int64_t)type_o * NC, px, py, pz,
-                                              cell);
+                                              deg == 2 ? ac42 : ac41, n0, n1, n2, accept_word(w),
+                                              omega + (int64_t)type_o * NC, px, py, pz, cell);
                     if (acc) { xo = px; yo = py; zo = pz; }
                     nacc += acc ? 1u : 0u;
                     if (MODE == kMoveGrid) {

@@ -108,6 +108,40 @@ __device__ __forceinline__ void normals3(uint4 w, float& n0, float& n1, float& n
     n2 = __fmul_rn(r1, c);
 }
 
+// normals3 that also returns the spare sine of its second Box-Muller pair
+// (the first normal of the next, odd, bead).
+__device__ __forceinline__ void normals3_spare(uint4 w, float& n0, float& n1, float& n2, float& spare) {
+    float s, c;
+    const float r0 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.x))));
+    sincos_turn(w.y, s, c);
+    n0 = __fmul_rn(r0, c);
+    n1 = __fmul_rn(r0, s);
+    const float r1 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.z))));
+    sincos_turn(w.w, s, c);
+    n2 = __fmul_rn(r1, c);
+    spare = __fmul_rn(r1, s);
+}
+
+// The spare sine of bead b-1's block, for an odd bead b whose even partner is
+// not at hand.
+__device__ __forceinline__ float spare_of(uint4 wp) {
+    float s, c;
+    const float r1 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(wp.z))));
+    sincos_turn(wp.w, s, c);
+    return __fmul_rn(r1, s);
+}
+
+// Normals of an odd bead: the spare sine of bead b-1, then Box-Muller on
+// (w.x, w.y) of its own block.  Three Box-Muller pairs per two beads.
+__device__ __forceinline__ void normals3_odd(float spare, uint4 w, float& n0, float& n1, float& n2) {
+    float s, c;
+    const float r = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.x))));
+    sincos_turn(w.y, s, c);
+    n0 = spare;
+    n1 = __fmul_rn(r, c);
+    n2 = __fmul_rn(r, s);
+}
+
 // The Metropolis uniform of a move: the low bytes of w.y, w.z, w.w of the
 // block that gave its normals (bits the normals never read).
 __device__ __forceinline__ uint32_t accept_word(uint4 w) {

@@ -13,9 +13,10 @@
  * Algorithm (one sweep at step s):
  *   for every chain, for colour c = 0 .. n_colours-1, for every bead b of
  *   colour c: a smart-MC (force-biased, Rossky-Doll-Friedman) trial against the
- *   frozen omega field.  One Philox4x32-10 block with counter (chain, b, s, 0)
- *   gives the three Gaussian displacement components and, from the bytes the
- *   normals do not read, the Metropolis uniform.
+ *   frozen omega field.  The Philox4x32-10 block with counter (chain, b, s, 0)
+ *   gives the Gaussian displacement of bead b (an odd bead also takes the
+ *   spare sine of bead b-1's block) and, from the bytes the normals do not
+ *   read, its Metropolis uniform.
  *   Bonded beads never share a colour, so the result does not depend on the
  *   order in which beads of one colour are visited, nor on chain order.
  * The reference instead draws `length` random beads with replacement per chain
@@ -130,6 +131,21 @@ void orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2) {
     float r1 = sqrtf(-2.0f * orc_logf(orc_u01(w[2])));
     orc_sincos_turn(w[3], &s, &c);
     *n2 = r1 * c;
+}
+
+/* Normals of an odd bead b: the first is the sine partner of bead b-1's third
+ * normal (the unused half of Box-Muller on (wp[2], wp[3]), wp = block of b-1);
+ * the other two are Box-Muller on (w[0], w[1]) of its own block.  Three
+ * Box-Muller pairs per two beads. */
+void orc_normals3_odd(const uint32_t wp[4], const uint32_t w[4], float* n0, float* n1, float* n2) {
+    float s, c;
+    float rb = sqrtf(-2.0f * orc_logf(orc_u01(wp[2])));
+    orc_sincos_turn(wp[3], &s, &c);
+    *n0 = rb * s;
+    float r = sqrtf(-2.0f * orc_logf(orc_u01(w[0])));
+    orc_sincos_turn(w[1], &s, &c);
+    *n1 = r * c;
+    *n2 = r * s;
 }
 
 /* The Metropolis uniform of a move comes from the same Philox block: the low
@@ -459,14 +475,21 @@ static inline int move_bead(const orc_system* s, const orc_arch* a, int b, float
     return acc;
 }
 
-/* One trial of bead b: its Philox block (chain, b, step, 0) gives the three
- * normals and the Metropolis word. */
+/* One trial of bead b: its Philox block (chain, b, step, 0) gives the
+ * Metropolis word and the normals (even b: normals3; odd b: see
+ * orc_normals3_odd, which also reads the block of bead b-1). */
 static inline int move_single(const orc_system* s, const orc_arch* a, uint32_t gc, int b,
                               float* X, float* Y, float* Z, const uint32_t key[2], uint32_t step) {
     uint32_t ctr[4] = {gc, (uint32_t)b, step, 0u}, w[4];
     orc_philox4x32_10(ctr, key, w);
     float n0, n1, n2;
-    orc_normals3(w, &n0, &n1, &n2);
+    if (b & 1) {
+        uint32_t cp[4] = {gc, (uint32_t)(b - 1), step, 0u}, wp[4];
+        orc_philox4x32_10(cp, key, wp);
+        orc_normals3_odd(wp, w, &n0, &n1, &n2);
+    } else {
+        orc_normals3(w, &n0, &n1, &n2);
+    }
     return move_bead(s, a, b, X, Y, Z, n0, n1, n2, orc_accept_word(w));
 }
 

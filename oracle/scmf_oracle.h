@@ -78,6 +78,7 @@ void  orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t o
 float orc_logf(float x);
 void  orc_sincos_turn(uint32_t w, float* s, float* c);
 void  orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2);
+void  orc_normals3_odd(const uint32_t wp[4], const uint32_t w[4], float* n0, float* n1, float* n2);
 float orc_u01(uint32_t w);
 uint32_t orc_accept_word(const uint32_t w[4]);
 int   orc_fold(float x, float inv_d, int n);
