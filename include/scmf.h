@@ -213,6 +213,84 @@ scmf_status scmf_read_coords_file(const char* path, int64_t skip_beads, float* x
  * grid point whatever the type count); 0 takes 2*n_types from the file. */
 scmf_status scmf_vtk_convert(const char* density_path, const char* vtk_path, int32_t values_per_point);
 
+/* ---------------------------------------------------- time-averaged density
+ * Replaces average_field_unified (struct.h:234, allocated at
+ * init_config.cu:770 and never filled) and io_out_aver_density (io.cpp:57-94).
+ * While averaging is on, every sweep s with s % every == 0 adds the counts of
+ * its final positions into a uint64 accumulator inside the fused field step
+ * (no extra pass over the counts). */
+/* every >= 1 starts (or restarts) averaging with a zeroed accumulator of
+ * 8 * n_types * n_cells bytes; every = 0 stops it and frees the accumulator. */
+scmf_status scmf_average_start(scmf_system* sys, uint32_t every);
+/* Adds the current counts as one sample now (for drivers that call the
+ * reference-shaped pieces instead of scmf_step). */
+scmf_status scmf_average_sample(scmf_system* sys);
+/* Sums [type][z][y][x] (n = n_types * n_cells) and the number of samples. */
+scmf_status scmf_average_get(const scmf_system* sys, uint64_t* sums, size_t n, uint64_t* n_samples);
+/* density_aver_<step>.dat (path NULL) in the density-file format: per cell the
+ * mean phi_T = (sum_T / n_samples) * n_cells / n_beads of every type, then the
+ * current omega_T, "%g " each. */
+scmf_status scmf_write_average_density(const scmf_system* sys, const char* path, int64_t step);
+
+/* ------------------------------------------------------------ checkpoints
+ * A binary checkpoint holds everything the next sweep reads: positions (FP32,
+ * bit for bit), omega, the step, the statistics and the averaging state, with
+ * a checksum.  Reading it into a system of the same spec resumes the run
+ * exactly (the random stream is stateless: it depends only on seed, chain,
+ * bead and step).  Counts are recomputed from the positions on reading.  The
+ * reference's restart (read_file=1, init_config.cu:930-987) goes through the
+ * lossy "%g" coord.dat and recomputes omega, so it does not resume exactly. */
+/* File layout (little endian): the 8 bytes "SCMFCKPT", this 128-byte header,
+ * then the payload: positions float[3 * n_beads] (AoS, the order of
+ * scmf_get_coords), omega float[n_types * n_cells], and when avg_every > 0 the
+ * accumulator uint64[n_types * n_cells]. */
+typedef struct scmf_checkpoint_header {
+    uint32_t version;         /* 1 */
+    int32_t n_types, nx, ny, nz;
+    int32_t n_chains, n_arch;
+    uint32_t avg_every;       /* 0: no accumulator stored */
+    int64_t n_beads;
+    int64_t n_cells;
+    uint64_t seed;
+    uint64_t spec_hash;       /* hash of every spec field that changes a trajectory (seed aside) */
+    uint64_t step;
+    uint64_t last_accepts, total_accepts, total_moves;
+    double e_field;
+    uint64_t avg_samples;
+    uint64_t payload_bytes;
+    uint64_t payload_hash;    /* FNV-1a 64 of the payload bytes */
+} scmf_checkpoint_header;
+scmf_status scmf_checkpoint_write(const scmf_system* sys, const char* path);
+scmf_status scmf_checkpoint_read(scmf_system* sys, const char* path);
+/* Reads and checks the header (and the payload checksum) without a system. */
+scmf_status scmf_checkpoint_info(const char* path, scmf_checkpoint_header* out);
+/* spec_hash a checkpoint of systems of this spec carries. */
+scmf_status scmf_spec_hash(const scmf_spec* spec, uint64_t* out);
+
+/* --------------------------------------------------------------- analysis
+ * Chain observables as device reductions (double), per architecture: the
+ * reference's end-to-end distance (test.cpp:47-68, beads 0 and 31 of every
+ * chain) generalised to first/last bead of any length, and the analyses its
+ * Ana_Info names (struct.h:65-75: Re, Rg, bond anisotropy, acceptance ratio,
+ * MSD) which it never computes. */
+typedef struct scmf_observables {
+    int32_t arch;             /* architecture index */
+    int32_t n_chains;
+    int64_t n_beads;
+    int64_t n_bonds;
+    double re2[4];            /* <R_e,x^2>, <R_e,y^2>, <R_e,z^2>, <|R_e|^2> over chains */
+    double rg2[4];            /* <R_g^2> components and total over chains */
+    double bond2[4];          /* <b_x^2>, <b_y^2>, <b_z^2>, <|b|^2> over bonds */
+    double msd[4];            /* bead <|r - r_ref|^2> components and total (NaN: no reference) */
+    double msd_com[4];        /* chain centre-of-mass displacement, same form */
+    double acc_ratio;         /* accepted / attempted moves of the last sweep (whole system) */
+    double reserved[3];
+} scmf_observables;
+/* Takes the current positions as the reference for displacements. */
+scmf_status scmf_analysis_reference(scmf_system* sys);
+/* Fills out[0 .. n_arch-1]; n_arch must equal the system's architecture count. */
+scmf_status scmf_analyze(const scmf_system* sys, scmf_observables* out, int32_t n_arch);
+
 /* -------------------------------------------------------------- batched */
 /* Many independent systems advanced together: one persistent kernel per
  * phase over a work list of (system, chain tile) and (system, cell tile),

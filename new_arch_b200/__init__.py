@@ -7,7 +7,7 @@ update with energy and acceptance reductions.
 """
 from ._lib import FIELD_EVERY, FIELD_REFERENCE, HAM_LITERAL, HAM_SCMF0, ScmfError, lib
 from .spec import Arch, SystemSpec
-from .system import Batch, System, read_coords_file, vtk_convert
+from .system import Batch, System, checkpoint_info, read_coords_file, vtk_convert
 
-__all__ = ["Arch", "SystemSpec", "System", "Batch", "ScmfError", "lib", "read_coords_file", "vtk_convert",
+__all__ = ["Arch", "SystemSpec", "System", "Batch", "ScmfError", "lib", "read_coords_file", "vtk_convert", "checkpoint_info",
            "FIELD_EVERY", "FIELD_REFERENCE", "HAM_SCMF0", "HAM_LITERAL"]

@@ -61,6 +61,21 @@ class Result(C.Structure):
                 ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
 
 
+class CheckpointHeader(C.Structure):
+    _fields_ = [("version", C.c_uint32), ("n_types", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32),
+                ("nz", C.c_int32), ("n_chains", C.c_int32), ("n_arch", C.c_int32), ("avg_every", C.c_uint32),
+                ("n_beads", C.c_int64), ("n_cells", C.c_int64), ("seed", C.c_uint64), ("spec_hash", C.c_uint64),
+                ("step", C.c_uint64), ("last_accepts", C.c_uint64), ("total_accepts", C.c_uint64),
+                ("total_moves", C.c_uint64), ("e_field", C.c_double), ("avg_samples", C.c_uint64),
+                ("payload_bytes", C.c_uint64), ("payload_hash", C.c_uint64)]
+
+
+class Observables(C.Structure):
+    _fields_ = [("arch", C.c_int32), ("n_chains", C.c_int32), ("n_beads", C.c_int64), ("n_bonds", C.c_int64),
+                ("re2", C.c_double * 4), ("rg2", C.c_double * 4), ("bond2", C.c_double * 4), ("msd", C.c_double * 4),
+                ("msd_com", C.c_double * 4), ("acc_ratio", C.c_double), ("reserved", C.c_double * 3)]
+
+
 # name -> (restype, argtypes)
 _vp, _i32, _i64, _u32, _u64, _sz, _f64 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_size_t, C.c_double
 _pvp = C.POINTER(C.c_void_p)
@@ -109,6 +124,16 @@ SIGNATURES = {
     "scmf_write_coords": (_i32, [_vp, C.c_char_p]),
     "scmf_read_coords_file": (_i32, [C.c_char_p, _i64, _pf32, _sz]),
     "scmf_vtk_convert": (_i32, [C.c_char_p, C.c_char_p, _i32]),
+    "scmf_average_start": (_i32, [_vp, _u32]),
+    "scmf_average_sample": (_i32, [_vp]),
+    "scmf_average_get": (_i32, [_vp, C.POINTER(C.c_uint64), _sz, C.POINTER(C.c_uint64)]),
+    "scmf_write_average_density": (_i32, [_vp, C.c_char_p, _i64]),
+    "scmf_checkpoint_write": (_i32, [_vp, C.c_char_p]),
+    "scmf_checkpoint_read": (_i32, [_vp, C.c_char_p]),
+    "scmf_checkpoint_info": (_i32, [C.c_char_p, C.POINTER(CheckpointHeader)]),
+    "scmf_spec_hash": (_i32, [_vp, C.POINTER(C.c_uint64)]),
+    "scmf_analysis_reference": (_i32, [_vp]),
+    "scmf_analyze": (_i32, [_vp, C.POINTER(Observables), _i32]),
     "scmf_batch_create": (_i32, [_pvp, _i32, C.POINTER(Tune), _vp, _pvp]),
     "scmf_batch_step": (_i32, [_vp, _i32]),
     "scmf_batch_step_async": (_i32, [_vp, _i32]),

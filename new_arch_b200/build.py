@@ -30,7 +30,7 @@ CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-result", "-ffp-
              "-I" + INC, "-I" + CSRC, "-I" + os.path.join(CUDA, "include")]
 
 CU_SOURCES = ["scmf_kernels.cu"]
-CXX_SOURCES = ["scmf_engine.cpp", "scmf_api.cpp", "scmf_files.cpp", "scmf_server.cpp"]
+CXX_SOURCES = ["scmf_engine.cpp", "scmf_api.cpp", "scmf_files.cpp", "scmf_server.cpp", "scmf_state.cpp"]
 HEADERS = ["scmf_internal.h", "scmf_math.cuh", "scmf_engine.h"]
 TOOLS = {"scmf": "scmf_cli.cpp", "scmf_vtk": "scmf_vtk_cli.cpp"}
 

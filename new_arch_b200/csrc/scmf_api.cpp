@@ -44,13 +44,22 @@ void free_system(scmf_system* s) {
     if (!s) return;
     s->plan.release();
     void* ptrs[] = {s->x, s->y, s->z, s->chain_id, s->counts[0], s->counts[1], s->omega, s->d_sys, s->d_arch,
-                    s->d_arch_blob, s->d_aos, s->d_u32};
+                    s->d_arch_blob, s->d_aos, s->d_u32, s->d_avg, s->d_ref, s->d_obs};
     for (void* p : ptrs) dev_free(p, s->stream);
     if (s->own_stream && s->stream) {
         cudaStreamSynchronize(s->stream);
         cudaStreamDestroy(s->stream);
     }
     delete s;
+}
+
+}  // namespace
+
+namespace scmf {
+
+scmf_status alloc_scratch(void** p, size_t bytes, cudaStream_t st) {
+    size_t dummy = 0;
+    return dalloc(p, bytes, &dummy, st);
 }
 
 size_t counts_bytes(const scmf_system* s) {
@@ -91,7 +100,7 @@ scmf_status check_error_word(const scmf_system* s) {
     return SCMF_OK;
 }
 
-}  // namespace
+}  // namespace scmf
 
 extern "C" {
 
@@ -431,7 +440,7 @@ scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float*
         if (!e) e = launch_field(true, 0, p.d_field, p.n_field, fs, p.d_ef, s->stream);
         if (!e)
             e = launch_close(p.d_close, p.n_sys, p.d_acc, p.warps_per_tile(), p.d_ef, p.d_eb,
-                             kCloseMove | kCloseField | kCloseFlip | kCloseAdvance, s->stream);
+                             kCloseMove | kCloseField | kCloseFlip | kCloseAdvance | kCloseAverage, s->stream);
         cudaEventRecord(ev[3 * i + 2], s->stream);
         if (e) rc = fail(SCMF_E_CUDA, "launch: %s", cudaGetErrorString((cudaError_t)e));
     }

@@ -6,8 +6,12 @@
 // (0) -Steps_N= (100) -read_file= (0), and writes density_<step>.dat every
 // Check_T steps, coord.dat at the end, and the "step %d end to end dis %g" /
 // "time =%g" lines.  Added flags: -seed= (default time(NULL), as
-// init_config.cu:864) and -field_rule=every.  One GPU only: -GPU_N > 1 is an
-// error (the multi-GPU density reduction of mesh.cu:10-81 is not built).
+// init_config.cu:864), -field_rule=every, -Aver_T=<n> (time-averaged density
+// over every n-th sweep, density_aver_<step>.dat beside each density file,
+// io.cpp:57-94), -checkpoint=1 (binary checkpoint.bin at the end) and
+// -read_file=2 (exact resume from checkpoint.bin, its step replacing
+// -Start_time).  One GPU only: -GPU_N > 1 is an error (the multi-GPU density
+// reduction of mesh.cu:10-81 is not built).
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -52,15 +56,20 @@ static const char* arg_str(int argc, char** argv, const char* name) {
         }                                                                          \
     } while (0)
 
-static double end_to_end(const std::vector<float>& xyz, const std::vector<std::pair<int, int>>& chains) {
-    double s = 0;
-    for (const auto& c : chains) {
-        const float* a = &xyz[3 * (size_t)c.first];
-        const float* b = &xyz[3 * (size_t)c.second];
-        const double dx = (double)a[0] - b[0], dy = (double)a[1] - b[1], dz = (double)a[2] - b[2];
-        s += dx * dx + dy * dy + dz * dz;
+// Mean squared end-to-end distance over all chains (test.cpp:47-68 averages
+// |r_0 - r_31|^2 over every chain), from the device reduction.
+static scmf_status end_to_end(const scmf_system* sys, int n_arch, double* out) {
+    std::vector<scmf_observables> o((size_t)n_arch);
+    scmf_status rc = scmf_analyze(sys, o.data(), n_arch);
+    if (rc) return rc;
+    double s = 0, n = 0;
+    for (const auto& v : o) {
+        if (v.n_chains == 0) continue;
+        s += v.re2[3] * v.n_chains;
+        n += v.n_chains;
     }
-    return chains.empty() ? 0.0 : s / chains.size();
+    *out = n > 0 ? s / n : 0.0;
+    return SCMF_OK;
 }
 
 int main(int argc, char** argv) {
@@ -77,6 +86,8 @@ int main(int argc, char** argv) {
     int nsteps = arg_int(argc, argv, "Steps_N", 0);
     if (nsteps == 0) nsteps = 100;
     const int read_file = arg_int(argc, argv, "read_file", 0);
+    const int aver_t = arg_int(argc, argv, "Aver_T", 0);
+    const int want_checkpoint = arg_int(argc, argv, "checkpoint", 0);
     bool seed_given = false;
     const int seed_arg = arg_int(argc, argv, "seed", 0, &seed_given);
     const uint64_t seed = seed_given ? (uint64_t)(uint32_t)seed_arg : (uint64_t)time(NULL);
@@ -96,16 +107,6 @@ int main(int argc, char** argv) {
     }
     scmf_spec_info info;
     TRY(scmf_spec_get_info(spec, &info));
-    std::vector<std::pair<int, int>> chains;  // first / last bead of every chain
-    {
-        int64_t base = 0;
-        for (int a = 0; a < info.n_arch; ++a) {
-            int32_t len = 0, nch = 0;
-            TRY(scmf_spec_get_arch(spec, a, &len, &nch, nullptr, 0, nullptr, 0, nullptr, nullptr));
-            for (int c = 0; c < nch; ++c) chains.push_back({(int)(base + (int64_t)c * len), (int)(base + (int64_t)c * len + len - 1)});
-            base += (int64_t)len * nch;
-        }
-    }
     scmf_system* sys = nullptr;
     TRY(scmf_system_create(spec, nullptr, &sys));
     TRY(scmf_init_coords(sys));
@@ -120,21 +121,48 @@ int main(int argc, char** argv) {
             TRY(scmf_set_coords(sys, xyz.data(), xyz.size()));
         }
     }
-    TRY(scmf_set_step(sys, (uint64_t)start));
     int step = start;
-    const int last = start + nsteps;
+    if (read_file == 2) {
+        FILE* f = fopen("checkpoint.bin", "rb");
+        if (!f) {
+            fprintf(stderr, "scmf: -read_file=2 needs checkpoint.bin\n");
+            return 1;
+        }
+        fclose(f);
+        TRY(scmf_checkpoint_read(sys, "checkpoint.bin"));
+        scmf_stats st;
+        TRY(scmf_get_sweep_stats(sys, &st));
+        step = (int)st.step;
+    } else {
+        TRY(scmf_set_step(sys, (uint64_t)start));
+    }
+    bool have_samples = false;  // the accumulator holds at least one sweep
+    const int aver_from = step;
+    if (aver_t > 0) {
+        scmf_checkpoint_header h;
+        // a resumed run keeps the checkpoint's accumulator when it averages at the same cadence
+        const bool keep = read_file == 2 && scmf_checkpoint_info("checkpoint.bin", &h) == SCMF_OK &&
+                          h.avg_every == (uint32_t)aver_t;
+        if (!keep) TRY(scmf_average_start(sys, (uint32_t)aver_t));
+        have_samples = keep && h.avg_samples > 0;
+    }
+    const int last = step + nsteps;
     while (step < last) {
         int next = ((step / tcheck) + 1) * tcheck;
         if (next > last) next = last;
         TRY(scmf_step(sys, next - step));
         step = next;
         if (step % tcheck == 0) {
-            TRY(scmf_get_coords(sys, xyz.data(), xyz.size()));
-            printf("step %d end to end dis %g\n", step, end_to_end(xyz, chains));
+            double ree = 0;
+            TRY(end_to_end(sys, info.n_arch, &ree));
+            printf("step %d end to end dis %g\n", step, ree);
             TRY(scmf_write_density(sys, nullptr, step));
+            if (aver_t > 0 && (have_samples || step / aver_t > aver_from / aver_t))
+                TRY(scmf_write_average_density(sys, nullptr, step));
         }
     }
     TRY(scmf_write_coords(sys, "coord.dat"));
+    if (want_checkpoint) TRY(scmf_checkpoint_write(sys, "checkpoint.bin"));
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);

@@ -336,7 +336,7 @@ scmf_status DevPlan::enqueue_close(int mode, cudaStream_t st) const {
 scmf_status DevPlan::enqueue_sweep(cudaStream_t st) const {
     CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, move_shape(), d_acc, st));
     CKL(launch_field(true, 0, d_field, n_field, field_shape(), d_ef, st));
-    return enqueue_close(kCloseMove | kCloseField | kCloseFlip | kCloseAdvance, st);
+    return enqueue_close(kCloseMove | kCloseField | kCloseFlip | kCloseAdvance | kCloseAverage, st);
 }
 
 scmf_status DevPlan::run_sweeps(cudaStream_t st, int n) {
@@ -397,7 +397,7 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
             mt.n_chains = std::min(cpt, A.n_chains - c);
             mt.bead0 = A.bead_base + (int64_t)c * A.length;
             mt.n_tiles_sys = 0;
-            mt.pad = 0;
+            mt.arch_index = (int32_t)a;
             p->move.push_back(mt);
             p->max_tile_beads = std::max(p->max_tile_beads, mt.n_chains * A.length);
             p->max_chains = std::max(p->max_chains, mt.n_chains);

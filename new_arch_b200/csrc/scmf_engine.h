@@ -117,6 +117,9 @@ struct scmf_system {
     void* d_arch_blob = nullptr;
     float* d_aos = nullptr;      // staging for AoS coordinate transfers (lazy)
     uint32_t* d_u32 = nullptr;   // staging for unpacked 16-bit counts (lazy)
+    unsigned long long* d_avg = nullptr;  // time-averaged density accumulator (while averaging)
+    float* d_ref = nullptr;      // reference snapshot for displacements, SoA (lazy)
+    double* d_obs = nullptr;     // per-tile observable partials (lazy)
     std::vector<scmf::ArchHost> archs;
     std::vector<scmf::ArchDev> h_arch;  // host image of d_arch
     scmf::DevPlan plan;                  // default work plan of this system alone
@@ -135,4 +138,11 @@ namespace scmf {
 scmf_status fetch_sysdev(const scmf_system* s, SysDev* out);
 scmf_status current_counts(const scmf_system* s, uint32_t* host_out, size_t n);
 scmf_status write_density_file(const scmf_system* s, const char* path, int64_t step);
+// scmf_api.cpp helpers shared with scmf_state.cpp
+scmf_status alloc_scratch(void** p, size_t bytes, cudaStream_t st);  // device buffer, 256-byte rounded
+size_t counts_bytes(const scmf_system* s);
+scmf_status regrid(scmf_system* s);         // counts of the current positions into counts[0], cur = 0
+scmf_status field_now(scmf_system* s);      // omega of the current counts (always updated)
+scmf_status ensure_aos(scmf_system* s);     // AoS staging buffer
+scmf_status check_error_word(const scmf_system* s);
 }  // namespace scmf

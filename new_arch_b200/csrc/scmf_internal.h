@@ -84,6 +84,12 @@ struct SysDev {
     double e_bond, e_field;
     uint32_t e_bond_step;  // step at which e_bond was last computed (+1; 0 = never)
     uint32_t pad1;
+    // time-averaged density (io.cpp:57-94): the fused sweep adds the new counts
+    // into avg at every sweep s with s % avg_every == 0 (avg NULL = off)
+    unsigned long long* avg;         // [n_types * n_cells]
+    unsigned long long avg_samples;  // sweeps accumulated
+    uint32_t avg_every;
+    uint32_t pad2;
 };
 
 // Work item of the move / grid kernel: a run of whole chains of one architecture.
@@ -94,7 +100,7 @@ struct MoveTile {
     int32_t n_chains;
     int64_t bead0;        // first bead (system arrays)
     int32_t n_tiles_sys;  // move tiles of this system in the launch
-    int32_t pad;
+    int32_t arch_index;   // architecture of the tile within its system
 };
 
 // Work item of the field kernel: a run of cells of one system.
@@ -108,7 +114,21 @@ struct FieldTile {
 enum SweepMode : int { kMoveOnly = 0, kMoveGrid = 1, kGridOnly = 2 };
 
 // What k_close does for each system of a launch.
-enum CloseMode : int { kCloseMove = 1, kCloseField = 2, kCloseBond = 4, kCloseFlip = 8, kCloseAdvance = 16 };
+enum CloseMode : int {
+    kCloseMove = 1, kCloseField = 2, kCloseBond = 4, kCloseFlip = 8, kCloseAdvance = 16,
+    kCloseAverage = 32  // count a time-averaged density sample when the sweep took one
+};
+
+// Per-tile partial sums of the chain observables (k_observables), each over
+// the chains of one move tile, in double.
+enum ObsSlot : int {
+    kObsRe = 0,     // end-to-end vector components squared, x y z (first to last bead)
+    kObsRg = 3,     // radius of gyration components squared
+    kObsBond = 6,   // bond vector components squared, summed over bonds
+    kObsMsd = 9,    // bead displacement from the reference snapshot, squared
+    kObsMsdCom = 12,  // chain centre-of-mass displacement, squared
+    kObsSlots = 16
+};
 
 // The tile ranges of one system in a launch's work lists.
 struct SysClose {
@@ -143,6 +163,12 @@ int launch_aos_to_soa(const float* aos, SysDev* sys, const ArchDev* arch, int n_
 int launch_soa_to_aos(float* aos, const SysDev* sys, const ArchDev* arch, int n_arch, int64_t n_beads,
                       void* stream);
 int launch_unpack_counts16(const SysDev* sys, uint32_t* out, int64_t n, void* stream);
+// Adds the current counts into SysDev::avg and counts one sample.
+int launch_average_sample(SysDev* sys, int64_t n, void* stream);
+// Chain observables: kObsSlots partial sums per move tile into part; ref_xyz
+// is the SoA reference snapshot (x, then y, then z; NULL = no displacements).
+int launch_observables(const MoveTile* tiles, int n_tiles, const float* ref_xyz, int64_t n_beads_sys,
+                       double* part, void* stream);
 size_t sweep_smem_bytes(int max_tile_beads, int max_length);
 // Field coefficients cf[t + n*s] in FP32 from xn[t + n*s] (double): diagonal
 // xn/N_ref; off-diagonal -xn/(2 N_ref) (SCMF0) or xn/N_ref (literal).

@@ -705,7 +705,7 @@ __device__ __forceinline__ double omega_of_cell(int nt, const uint32_t* cnt, flo
 template <int NT, bool FUSED>
 __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, float scale, bool lit, bool upd,
                                              bool c16, const uint32_t* src32, uint32_t* clr32, float* W,
-                                             const float* cf) {
+                                             const float* cf, unsigned long long* avg) {
     constexpr int M = NT > 0 ? NT : kMaxTypes;
     const int nt = NT > 0 ? NT : n;
     const uint16_t* src16 = reinterpret_cast<const uint16_t*>(src32);
@@ -717,6 +717,7 @@ __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, fl
         if (u < nt) {
             cnt[u] = c16 ? (uint32_t)src16[u * NC + cell] : src32[u * NC + cell];
             if (!upd) w[u] = W[u * NC + cell];
+            if (avg) avg[u * NC + cell] += cnt[u];
         }
     }
     const double ef = omega_of_cell<NT>(nt, cnt, scale, lit, upd, w, cf);
@@ -739,13 +740,25 @@ __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, fl
 // counts, n_cells and the tile start multiples of 4).
 template <int NT, bool FUSED>
 __device__ __forceinline__ double field_cells4(int64_t cell, int64_t NC, float scale, bool lit, bool upd,
-                                               const uint32_t* src32, uint32_t* clr32, float* W, const float* cf) {
+                                               const uint32_t* src32, uint32_t* clr32, float* W, const float* cf,
+                                               unsigned long long* avg) {
     uint4 cv[NT];
     float4 wv[NT];
 #pragma unroll
     for (int u = 0; u < NT; ++u) {
         cv[u] = __ldcs(reinterpret_cast<const uint4*>(src32 + u * NC + cell));
         if (!upd) wv[u] = *reinterpret_cast<const float4*>(W + u * NC + cell);
+    }
+    if (avg) {
+#pragma unroll
+        for (int u = 0; u < NT; ++u) {
+            ulonglong2* a = reinterpret_cast<ulonglong2*>(avg + u * NC + cell);
+            ulonglong2 lo = a[0], hi = a[1];
+            lo.x += cv[u].x; lo.y += cv[u].y;
+            hi.x += cv[u].z; hi.y += cv[u].w;
+            a[0] = lo;
+            a[1] = hi;
+        }
     }
     double ef = 0.0;
 #pragma unroll
@@ -796,14 +809,16 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
         const uint32_t* src32 = S->counts[FUSED ? (cur ^ 1u) : cur];
         uint32_t* clr32 = FUSED ? S->counts[cur] : nullptr;
         float* W = S->omega;
+        // the fused sweep samples the time-averaged density at every avg_every-th sweep
+        unsigned long long* avg = FUSED && S->avg && S->avg_every && (sweep % S->avg_every) == 0u ? S->avg : nullptr;
         double ef = 0.0;
         const int64_t end = t.cell0 + t.n_cells;
         if (NT > 0 && !c16 && (NC & 3) == 0 && (t.cell0 & 3) == 0 && (t.n_cells & 3) == 0) {
             for (int64_t cell = t.cell0 + 4 * tid; cell < end; cell += 4 * T)
-                ef += field_cells4<(NT > 0 ? NT : 1), FUSED>(cell, NC, scale, lit, upd, src32, clr32, W, cf);
+                ef += field_cells4<(NT > 0 ? NT : 1), FUSED>(cell, NC, scale, lit, upd, src32, clr32, W, cf, avg);
         } else {
             for (int64_t cell = t.cell0 + tid; cell < end; cell += T)
-                ef += field_cell<NT, FUSED>(n, cell, NC, scale, lit, upd, c16, src32, clr32, W, cf);
+                ef += field_cell<NT, FUSED>(n, cell, NC, scale, lit, upd, c16, src32, clr32, W, cf, avg);
         }
         ef = warp_sum(ef);
         if (lane == 0) s_ef[warp] = ef;
@@ -861,6 +876,8 @@ __global__ void __launch_bounds__(256) k_close(const SysClose* __restrict__ list
                 S->e_bond = s_f[0];
                 S->e_bond_step = S->step + 1u;
             }
+            if ((mode & kCloseAverage) && S->avg && S->avg_every && ((S->step + 1u) % S->avg_every) == 0u)
+                S->avg_samples += 1ull;
             if (mode & kCloseFlip) S->cur ^= 1u;
             if (mode & kCloseAdvance) S->step += 1u;
         }
@@ -904,6 +921,101 @@ __global__ void __launch_bounds__(256) k_bond_energy(const MoveTile* __restrict_
             double a = 0.0;
             for (int w = 0; w < (T + 31) / 32; ++w) a += s_e[w];
             eb_part[ti] = a;
+        }
+        __syncthreads();
+    }
+}
+
+// Adds the current counts into the time-averaged density accumulator and
+// counts the sample (a sample taken outside the fused sweep).
+__global__ void k_average_sample(SysDev* S, int64_t n) {
+    const uint32_t* c32 = S->counts[S->cur];
+    const uint16_t* c16 = reinterpret_cast<const uint16_t*>(c32);
+    const bool half = S->count16 != 0;
+    unsigned long long* avg = S->avg;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        avg[i] += half ? (unsigned long long)c16[i] : (unsigned long long)c32[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->avg_samples += 1ull;
+}
+
+// Chain observables in double, one warp per chain and one partial row of
+// kObsSlots sums per move tile (fixed reduction order).  Per chain:
+// R_e = last bead - first bead (test.cpp:47-68 takes beads 0 and 31 of every
+// chain); R_g^2 = mean |r - r_cm|^2; bonds counted once (j > i); with a
+// reference snapshot, bead and centre-of-mass displacements.  Ana_Info
+// (struct.h:65-75) names these analyses; the reference computes only R_e.
+__global__ void __launch_bounds__(256) k_observables(const MoveTile* __restrict__ tiles, int n_tiles,
+                                                      const float* __restrict__ ref, int64_t n_beads_sys,
+                                                      double* __restrict__ part) {
+    __shared__ double s_w[kMaxWarps][kObsSlots];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
+        const MoveTile t = tiles[ti];
+        const SysDev* S = t.sys;
+        const ArchDev* Ap = t.arch;
+        const int L = Ap->length;
+        double acc[kObsSlots];
+#pragma unroll
+        for (int k = 0; k < kObsSlots; ++k) acc[k] = 0.0;
+        for (int cl = warp; cl < t.n_chains; cl += nwarps) {
+            const int64_t b0 = t.bead0 + (int64_t)cl * L;
+            const float* X = S->x + b0;
+            const float* Y = S->y + b0;
+            const float* Z = S->z + b0;
+            double sx = 0.0, sy = 0.0, sz = 0.0, rx = 0.0, ry = 0.0, rz = 0.0;
+            double bx = 0.0, by = 0.0, bz = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+            for (int b = lane; b < L; b += 32) {
+                const double x = X[b], y = Y[b], z = Z[b];
+                sx += x; sy += y; sz += z;
+                const BeadInfo bi = Ap->beads[b];
+                for (int d = 0; d < bi.deg; ++d) {
+                    const int j = bi.nbr[d];
+                    if (j <= b) continue;
+                    const double ex = (double)X[j] - x, ey = (double)Y[j] - y, ez = (double)Z[j] - z;
+                    bx += ex * ex; by += ey * ey; bz += ez * ez;
+                }
+                if (ref) {
+                    const double ux = x - (double)ref[b0 + b], uy = y - (double)ref[n_beads_sys + b0 + b],
+                                 uz = z - (double)ref[2 * n_beads_sys + b0 + b];
+                    mx += ux * ux; my += uy * uy; mz += uz * uz;
+                    rx += (double)ref[b0 + b];
+                    ry += (double)ref[n_beads_sys + b0 + b];
+                    rz += (double)ref[2 * n_beads_sys + b0 + b];
+                }
+            }
+            sx = warp_sum(sx); sy = warp_sum(sy); sz = warp_sum(sz);
+            const double cx = sx / L, cy = sy / L, cz = sz / L;
+            double gx = 0.0, gy = 0.0, gz = 0.0;
+            for (int b = lane; b < L; b += 32) {
+                const double ux = (double)X[b] - cx, uy = (double)Y[b] - cy, uz = (double)Z[b] - cz;
+                gx += ux * ux; gy += uy * uy; gz += uz * uz;
+            }
+            gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz);
+            bx = warp_sum(bx); by = warp_sum(by); bz = warp_sum(bz);
+            if (ref) {
+                mx = warp_sum(mx); my = warp_sum(my); mz = warp_sum(mz);
+                rx = warp_sum(rx); ry = warp_sum(ry); rz = warp_sum(rz);
+            }
+            if (lane == 0) {
+                const double ex = (double)X[L - 1] - (double)X[0], ey = (double)Y[L - 1] - (double)Y[0],
+                             ez = (double)Z[L - 1] - (double)Z[0];
+                acc[kObsRe] += ex * ex; acc[kObsRe + 1] += ey * ey; acc[kObsRe + 2] += ez * ez;
+                acc[kObsRg] += gx / L; acc[kObsRg + 1] += gy / L; acc[kObsRg + 2] += gz / L;
+                acc[kObsBond] += bx; acc[kObsBond + 1] += by; acc[kObsBond + 2] += bz;
+                if (ref) {
+                    acc[kObsMsd] += mx; acc[kObsMsd + 1] += my; acc[kObsMsd + 2] += mz;
+                    const double dx = cx - rx / L, dy = cy - ry / L, dz = cz - rz / L;
+                    acc[kObsMsdCom] += dx * dx; acc[kObsMsdCom + 1] += dy * dy; acc[kObsMsdCom + 2] += dz * dz;
+                }
+            }
+        }
+        if (lane == 0)
+            for (int k = 0; k < kObsSlots; ++k) s_w[warp][k] = acc[k];
+        __syncthreads();
+        if (tid < kObsSlots) {
+            double a = 0.0;
+            for (int w = 0; w < nwarps; ++w) a += s_w[w][tid];
+            part[(int64_t)ti * kObsSlots + tid] = a;
         }
         __syncthreads();
     }
@@ -1100,6 +1212,17 @@ int launch_unpack_counts16(const SysDev* sys, uint32_t* out, int64_t n, void* st
     k_unpack16<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(sys, out, n);
     return (int)cudaGetLastError();
 }
+int launch_average_sample(SysDev* sys, int64_t n, void* stream) {
+    if (n <= 0) return 0;
+    k_average_sample<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(sys, n);
+    return (int)cudaGetLastError();
+}
+int launch_observables(const MoveTile* tiles, int n_tiles, const float* ref_xyz, int64_t n_beads_sys, double* part,
+                       void* stream) {
+    if (n_tiles <= 0) return 0;
+    k_observables<<<n_tiles, 256, 0, (cudaStream_t)stream>>>(tiles, n_tiles, ref_xyz, n_beads_sys, part);
+    return (int)cudaGetLastError();
+}
 
 }  // namespace scmf
 
@@ -1143,7 +1266,7 @@ __global__ void __launch_bounds__(256) k_field_noalloc(const uint32_t* __restric
     double ef = 0.0;
     for (int64_t cell = c0 + tid; cell < c1; cell += T)
         ef += field_cell<0, false>(p.n_types, cell, p.n_cells, p.scale, p.lit != 0, true, false, counts, nullptr,
-                                   omega, cf);
+                                   omega, cf, nullptr);
     ef = warp_sum(ef);
     if (lane == 0) s_ef[warp] = ef;
     __syncthreads();

@@ -40,6 +40,7 @@ class System:
         self.n_cells = info.n_cells
         self.n_types = info.n_types
         self.n_chains = info.n_chains
+        self.n_arch = info.n_arch
 
     # -------------------------------------------------------------- lifetime
     def close(self) -> None:
@@ -145,6 +146,56 @@ class System:
 
     def io_out_coord(self, path: str = "coord.dat") -> None:
         check(lib().scmf_write_coords(self._h, path.encode()))
+
+    # --------------------------------------------- time-averaged density
+    def average_start(self, every: int = 1) -> None:
+        """Sum the counts of every sweep s with s % every == 0 (0 stops)."""
+        check(lib().scmf_average_start(self._h, int(every)))
+
+    def average_sample(self) -> None:
+        check(lib().scmf_average_sample(self._h))
+
+    def average(self):
+        """(sums uint64 [n_types * n_cells], number of samples)"""
+        out = np.empty(self.n_types * self.n_cells, dtype=np.uint64)
+        n = C.c_uint64()
+        check(lib().scmf_average_get(self._h, _ptr(out, C.c_uint64), out.size, C.byref(n)))
+        return out, n.value
+
+    def io_out_aver_density(self, step: int, path: Optional[str] = None) -> None:
+        check(lib().scmf_write_average_density(self._h, path.encode() if path else None, int(step)))
+
+    # ------------------------------------------------------- checkpoints
+    def checkpoint_write(self, path: str) -> None:
+        check(lib().scmf_checkpoint_write(self._h, path.encode()))
+
+    def checkpoint_read(self, path: str) -> None:
+        check(lib().scmf_checkpoint_read(self._h, path.encode()))
+
+    # ---------------------------------------------------------- analysis
+    def analysis_reference(self) -> None:
+        """Current positions become the origin of the displacements."""
+        check(lib().scmf_analysis_reference(self._h))
+
+    def analyze(self) -> list:
+        """Per architecture: re2, rg2, bond2, msd, msd_com as (x, y, z, total)
+        means, plus n_chains, n_beads, n_bonds and the acceptance ratio."""
+        n = self.n_arch
+        arr = (_lib.Observables * n)()
+        check(lib().scmf_analyze(self._h, arr, n))
+        out = []
+        for o in arr:
+            d = {k: np.array(list(getattr(o, k))) for k in ("re2", "rg2", "bond2", "msd", "msd_com")}
+            d.update(arch=o.arch, n_chains=o.n_chains, n_beads=o.n_beads, n_bonds=o.n_bonds, acc_ratio=o.acc_ratio)
+            out.append(d)
+        return out
+
+
+def checkpoint_info(path: str) -> dict:
+    """Header of a checkpoint file, after checking its magic, sizes and checksum."""
+    h = _lib.CheckpointHeader()
+    check(lib().scmf_checkpoint_info(path.encode(), C.byref(h)))
+    return {k: getattr(h, k) for k, _ in _lib.CheckpointHeader._fields_}
 
 
 def read_coords_file(path: str, n_beads: int, skip: int = 0) -> np.ndarray:

@@ -66,6 +66,13 @@ def lib():
     L.orc_get_omega.argtypes = [vp, f32p]
     L.orc_set_omega.argtypes = [vp, f32p]
     L.orc_get_stats.argtypes = [vp, C.POINTER(OrcStats)]
+    L.orc_average_start.argtypes = [vp, C.c_uint32]
+    L.orc_average_sample.argtypes = [vp]
+    L.orc_average_get.restype = C.c_uint64
+    L.orc_average_get.argtypes = [vp, C.POINTER(C.c_uint64)]
+    L.orc_analysis_reference.argtypes = [vp]
+    L.orc_analyze.restype = i32
+    L.orc_analyze.argtypes = [vp, i32, C.POINTER(C.c_double)]
     L.orc_philox4x32_10.argtypes = [u32p, u32p, u32p]
     L.orc_logf.restype = C.c_float
     L.orc_logf.argtypes = [C.c_float]
@@ -195,3 +202,26 @@ class OracleSystem:
         st = OrcStats()
         lib().orc_get_stats(self._h, C.byref(st))
         return {k: getattr(st, k) for k, _ in OrcStats._fields_}
+
+    def average_start(self, every):
+        lib().orc_average_start(self._h, int(every))
+
+    def average_sample(self):
+        lib().orc_average_sample(self._h)
+
+    def average(self):
+        """(sums uint64 [n_types * n_cells], number of samples)"""
+        out = np.zeros(self.n_types * self.n_cells, dtype=np.uint64)
+        n = lib().orc_average_get(self._h, _p(out, C.c_uint64))
+        return out, int(n)
+
+    def analysis_reference(self):
+        lib().orc_analysis_reference(self._h)
+
+    def analyze(self, arch):
+        """Means of re2, rg2, bond2, msd, msd_com per component (x, y, z)."""
+        out = np.empty(15, dtype=np.float64)
+        if lib().orc_analyze(self._h, int(arch), _p(out, C.c_double)) != 0:
+            raise ValueError("oracle: no such architecture")
+        v = out.reshape(5, 3)
+        return {k: v[i] for i, k in enumerate(("re2", "rg2", "bond2", "msd", "msd_com"))}

@@ -203,6 +203,11 @@ struct orc_system {
     uint64_t step;
     orc_stats st;
     int finalized;
+    /* time-averaged density (io.cpp:57-94) and the displacement reference */
+    uint64_t* avg;
+    uint32_t avg_every;
+    uint64_t avg_samples;
+    float *rx, *ry, *rz;
 };
 
 static int g_threads = 1;
@@ -318,6 +323,7 @@ void orc_destroy(orc_system* s) {
     }
     free(s->x); free(s->y); free(s->z); free(s->counts); free(s->omega);
     free(s->chain_acc);
+    free(s->avg); free(s->rx); free(s->ry); free(s->rz);
     free(s);
 }
 
@@ -597,7 +603,101 @@ void orc_step(orc_system* s, int n) {
         orc_reset_density(s);
         int upd = (s->field_rule == 1) || (s->step % 10 != 0);
         field_update(s, upd);
+        if (s->avg && s->step % s->avg_every == 0) orc_average_sample(s);
     }
+}
+
+/* Time-averaged density: the counts of the final positions of every sweep s
+ * with s % every == 0 are summed (average_field_unified, struct.h:234). */
+void orc_average_start(orc_system* s, uint32_t every) {
+    free(s->avg);
+    s->avg = NULL;
+    s->avg_every = every;
+    s->avg_samples = 0;
+    if (every) s->avg = (uint64_t*)calloc((size_t)(s->n_cells * s->n_types), sizeof(uint64_t));
+}
+
+void orc_average_sample(orc_system* s) {
+    if (!s->avg) return;
+    const int64_t n = s->n_cells * s->n_types;
+    for (int64_t i = 0; i < n; ++i) s->avg[i] += s->counts[i];
+    s->avg_samples += 1;
+}
+
+uint64_t orc_average_get(const orc_system* s, uint64_t* sums) {
+    if (!s->avg) return 0;
+    memcpy(sums, s->avg, sizeof(uint64_t) * (size_t)(s->n_cells * s->n_types));
+    return s->avg_samples;
+}
+
+/* Chain observables in double.  R_e = last bead - first bead (test.cpp:47-68
+ * uses beads 0 and 31); R_g^2 = mean |r - r_cm|^2 per chain; bonds once
+ * (j > i); bead and centre-of-mass displacements from the reference
+ * snapshot.  out[15] = means of re2 xyz, rg2 xyz, bond2 xyz (per bond),
+ * msd xyz (per bead), msd_com xyz (per chain); NaN where undefined. */
+void orc_analysis_reference(orc_system* s) {
+    size_t nb = (size_t)s->n_beads;
+    if (!s->rx) {
+        s->rx = (float*)malloc(nb * sizeof(float));
+        s->ry = (float*)malloc(nb * sizeof(float));
+        s->rz = (float*)malloc(nb * sizeof(float));
+    }
+    memcpy(s->rx, s->x, nb * sizeof(float));
+    memcpy(s->ry, s->y, nb * sizeof(float));
+    memcpy(s->rz, s->z, nb * sizeof(float));
+}
+
+int orc_analyze(const orc_system* s, int arch, double* out) {
+    if (arch < 0 || arch >= s->n_arch) return -1;
+    const orc_arch* a = &s->arch[arch];
+    const int L = a->length;
+    double acc[15] = {0};
+    int64_t n_bonds = 0;
+    for (int c = 0; c < a->n_chains; ++c) {
+        const int64_t b0 = a->bead_base + (int64_t)c * L;
+        const float *X = s->x + b0, *Y = s->y + b0, *Z = s->z + b0;
+        double cx = 0, cy = 0, cz = 0, rcx = 0, rcy = 0, rcz = 0;
+        for (int b = 0; b < L; ++b) { cx += X[b]; cy += Y[b]; cz += Z[b]; }
+        cx /= L; cy /= L; cz /= L;
+        double gx = 0, gy = 0, gz = 0;
+        for (int b = 0; b < L; ++b) {
+            double ux = (double)X[b] - cx, uy = (double)Y[b] - cy, uz = (double)Z[b] - cz;
+            gx += ux * ux; gy += uy * uy; gz += uz * uz;
+        }
+        double ex = (double)X[L - 1] - (double)X[0], ey = (double)Y[L - 1] - (double)Y[0], ez = (double)Z[L - 1] - (double)Z[0];
+        acc[0] += ex * ex; acc[1] += ey * ey; acc[2] += ez * ez;
+        acc[3] += gx / L; acc[4] += gy / L; acc[5] += gz / L;
+        for (int b = 0; b < L; ++b)
+            for (int d = 0; d < a->deg[b]; ++d) {
+                int j = a->nbr[b * ORC_MAX_DEG + d];
+                if (j <= b) continue;
+                double bx = (double)X[j] - (double)X[b], by = (double)Y[j] - (double)Y[b], bz = (double)Z[j] - (double)Z[b];
+                acc[6] += bx * bx; acc[7] += by * by; acc[8] += bz * bz;
+                if (c == 0) n_bonds += 1;
+            }
+        if (s->rx) {
+            for (int b = 0; b < L; ++b) {
+                double ux = (double)X[b] - (double)s->rx[b0 + b], uy = (double)Y[b] - (double)s->ry[b0 + b],
+                       uz = (double)Z[b] - (double)s->rz[b0 + b];
+                acc[9] += ux * ux; acc[10] += uy * uy; acc[11] += uz * uz;
+                rcx += s->rx[b0 + b]; rcy += s->ry[b0 + b]; rcz += s->rz[b0 + b];
+            }
+            double dx = cx - rcx / L, dy = cy - rcy / L, dz = cz - rcz / L;
+            acc[12] += dx * dx; acc[13] += dy * dy; acc[14] += dz * dz;
+        }
+    }
+    const double nan = 0.0 / 0.0;
+    const double nc = a->n_chains ? (double)a->n_chains : nan;
+    const double nbd = n_bonds ? (double)n_bonds * a->n_chains : nan;
+    const double nbe = a->n_chains ? (double)a->n_chains * L : nan;
+    for (int k = 0; k < 3; ++k) {
+        out[k] = acc[k] / nc;
+        out[3 + k] = acc[3 + k] / nc;
+        out[6 + k] = acc[6 + k] / nbd;
+        out[9 + k] = s->rx ? acc[9 + k] / nbe : nan;
+        out[12 + k] = s->rx ? acc[12 + k] / nc : nan;
+    }
+    return 0;
 }
 
 /* Statistics; the bond energy is that of the current positions, computed on

@@ -73,6 +73,17 @@ void orc_get_omega(const orc_system* s, float* out);
 void orc_set_omega(orc_system* s, const float* in);
 void orc_get_stats(const orc_system* s, orc_stats* out);
 
+/* time-averaged density: orc_step adds the counts of every sweep s with
+ * s % every == 0 (every = 0 stops); orc_average_get returns the sample count */
+void     orc_average_start(orc_system* s, uint32_t every);
+void     orc_average_sample(orc_system* s);
+uint64_t orc_average_get(const orc_system* s, uint64_t* sums);
+
+/* chain observables (means in double): out[15] = re2 xyz, rg2 xyz, bond2 xyz,
+ * msd xyz, msd_com xyz; displacements are NaN before orc_analysis_reference */
+void orc_analysis_reference(orc_system* s);
+int  orc_analyze(const orc_system* s, int arch, double* out);
+
 /* math building blocks (exported for known-answer tests) */
 void  orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 float orc_logf(float x);

@@ -182,3 +182,33 @@ def test_full_size_properties(nb, which):
     set_threads(1)
     assert_counts_equal(cnt, o.counts(), which + " recount")
     assert_close(om, o.omega(), what=which + " omega")
+
+
+def test_cli_checkpoint_resume_and_average(nb, tmp_path):
+    """-checkpoint=1 then -read_file=2 continues exactly: coord.dat after 10 + 10
+    steps equals coord.dat after 20 uninterrupted steps (byte for byte), and
+    -Aver_T writes density_aver_<step>.dat beside each density file."""
+    exe = os.path.join(ROOT, "new_arch_b200", "_lib", "scmf")
+    a, b = tmp_path / "split", tmp_path / "whole"
+    for d in (a, b):
+        d.mkdir()
+        shutil.copy(os.path.join(GOLDEN, "configuration.dat"), d)
+        shutil.copy(os.path.join(GOLDEN, "polymer.dat"), d)
+    run = lambda d, *args: subprocess.run([exe, "-seed=5", "-Check_T=10", *args], cwd=d, capture_output=True,
+                                          text=True, timeout=300)
+    r = run(a, "-Steps_N=10", "-checkpoint=1", "-Aver_T=2")
+    assert r.returncode == 0, r.stderr
+    assert (a / "checkpoint.bin").exists() and (a / "density_aver_10.dat").exists()
+    info = nb.checkpoint_info(str(a / "checkpoint.bin"))
+    assert info["step"] == 10 and info["avg_every"] == 2 and info["avg_samples"] == 5
+    r = run(a, "-Steps_N=10", "-read_file=2", "-Aver_T=2")
+    assert r.returncode == 0, r.stderr
+    assert "step 20 end to end dis" in r.stdout
+    r = run(b, "-Steps_N=20", "-Aver_T=2")
+    assert r.returncode == 0, r.stderr
+    assert filecmp.cmp(a / "coord.dat", b / "coord.dat", shallow=False)
+    assert filecmp.cmp(a / "density_20.dat", b / "density_20.dat", shallow=False)
+    assert filecmp.cmp(a / "density_aver_20.dat", b / "density_aver_20.dat", shallow=False)
+    # the end-to-end line is the device reduction of the same positions
+    line_a = [l for l in r.stdout.splitlines() if l.startswith("step 20 end")]
+    assert line_a
