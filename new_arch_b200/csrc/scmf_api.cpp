@@ -83,8 +83,8 @@ scmf_status regrid(scmf_system* s) {
 scmf_status field_now(scmf_system* s) {
     LaunchShape sh = s->plan.field_shape();
     sh.blocks = 0;
-    CKL(launch_field(false, 1, s->plan.d_field, s->plan.n_field, sh, s->plan.d_ef, s->stream));
-    return s->plan.enqueue_close(kCloseField, s->stream);
+    CKL(launch_field(false, 1, s->plan.d_field, s->plan.n_field, sh, s->plan.d_ef, kCloseField, s->stream));
+    return SCMF_OK;
 }
 
 scmf_status ensure_aos(scmf_system* s) {
@@ -437,10 +437,7 @@ scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float*
         cudaEventRecord(ev[3 * i], s->stream);
         int e = launch_sweep(kMoveGrid, p.d_move, p.n_move, p.max_tile_beads, p.max_length, ms, p.d_acc, s->stream);
         cudaEventRecord(ev[3 * i + 1], s->stream);
-        if (!e) e = launch_field(true, 0, p.d_field, p.n_field, fs, p.d_ef, s->stream);
-        if (!e)
-            e = launch_close(p.d_close, p.n_sys, p.d_acc, p.warps_per_tile(), p.d_ef, p.d_eb,
-                             kCloseMove | kCloseField | kCloseFlip | kCloseAdvance | kCloseAverage, s->stream);
+        if (!e) e = launch_field(true, 0, p.d_field, p.n_field, fs, p.d_ef, kSweepClose, s->stream);
         cudaEventRecord(ev[3 * i + 2], s->stream);
         if (e) rc = fail(SCMF_E_CUDA, "launch: %s", cudaGetErrorString((cudaError_t)e));
     }

@@ -335,8 +335,8 @@ scmf_status DevPlan::enqueue_close(int mode, cudaStream_t st) const {
 
 scmf_status DevPlan::enqueue_sweep(cudaStream_t st) const {
     CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, move_shape(), d_acc, st));
-    CKL(launch_field(true, 0, d_field, n_field, field_shape(), d_ef, st));
-    return enqueue_close(kCloseMove | kCloseField | kCloseFlip | kCloseAdvance | kCloseAverage, st);
+    CKL(launch_field(true, 0, d_field, n_field, field_shape(), d_ef, kSweepClose, st));
+    return SCMF_OK;
 }
 
 scmf_status DevPlan::run_sweeps(cudaStream_t st, int n) {
@@ -417,6 +417,8 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
         ft.cell0 = (int64_t)i * cpt_cells;
         ft.n_cells = (int)std::min<int64_t>(cpt_cells, n_cells - ft.cell0);
         ft.n_tiles_sys = ntile;
+        ft.first_tile = (int32_t)first_field;
+        ft.pad = 0;
         p->field.push_back(ft);
     }
     SysClose cl;

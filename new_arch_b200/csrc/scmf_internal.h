@@ -89,7 +89,7 @@ struct SysDev {
     unsigned long long* avg;         // [n_types * n_cells]
     unsigned long long avg_samples;  // sweeps accumulated
     uint32_t avg_every;
-    uint32_t pad2;
+    uint32_t field_done;  // field tiles of the running launch finished (the last one closes the sweep)
 };
 
 // Work item of the move / grid kernel: a run of whole chains of one architecture.
@@ -109,6 +109,8 @@ struct FieldTile {
     int64_t cell0;
     int32_t n_cells;
     int32_t n_tiles_sys;  // field tiles of this system in the launch
+    int32_t first_tile;   // index of this system's first field tile in the launch
+    int32_t pad;
 };
 
 enum SweepMode : int { kMoveOnly = 0, kMoveGrid = 1, kGridOnly = 2 };
@@ -116,7 +118,8 @@ enum SweepMode : int { kMoveOnly = 0, kMoveGrid = 1, kGridOnly = 2 };
 // What k_close does for each system of a launch.
 enum CloseMode : int {
     kCloseMove = 1, kCloseField = 2, kCloseBond = 4, kCloseFlip = 8, kCloseAdvance = 16,
-    kCloseAverage = 32  // count a time-averaged density sample when the sweep took one
+    kCloseAverage = 32,  // count a time-averaged density sample when the sweep took one
+    kSweepClose = kCloseMove | kCloseField | kCloseFlip | kCloseAdvance | kCloseAverage
 };
 
 // Per-tile partial sums of the chain observables (k_observables), each over
@@ -153,8 +156,10 @@ int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_c
 // kernel one per move tile into eb_part; k_close sums and publishes them.
 int launch_sweep(int mode, const MoveTile* tiles, int n_tiles, int max_tile_beads, int max_length,
                  LaunchShape shape, unsigned* acc_part, void* stream);
+// close_mode != 0: the last field tile of every system closes it in the same
+// launch (what k_close does with that mode), so a sweep is two launches.
 int launch_field(bool fused, int force_update, const FieldTile* tiles, int n_tiles, LaunchShape shape,
-                 double* ef_part, void* stream);
+                 double* ef_part, int close_mode, void* stream);
 int launch_bond_energy(const MoveTile* tiles, int n_tiles, LaunchShape shape, double* eb_part, void* stream);
 int launch_close(const SysClose* list, int n_sys, const unsigned* acc_part, int warps_per_tile,
                  const double* ef_part, const double* eb_part, int mode, void* stream);

@@ -787,11 +787,59 @@ __device__ __forceinline__ double field_cells4(int64_t cell, int64_t NC, float s
     return ef;
 }
 
+// Closes one system after a launch (one block): sums the accept slots and the
+// energy partials part[0 .. count) in an order fixed by the block size, and
+// thread 0 publishes the statistics and, for a full sweep, advances the step
+// and makes the new counts current.  Partials written by other blocks of the
+// same launch are read through L2.
+__device__ void close_system(SysDev* S, const double* part, int count, int mode, unsigned long long* s_a,
+                             double* s_f) {
+    const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    unsigned long long a = 0;
+    double f = 0.0;
+    if ((mode & kCloseMove) && tid < kSlots) {
+        a = __ldcg(&S->slot_acc[tid]);
+        S->slot_acc[tid] = 0ull;
+    }
+    if (mode & (kCloseField | kCloseBond))
+        for (int i = tid; i < count; i += T) f += __ldcg(part + i);
+    a = warp_sum(a);
+    f = warp_sum(f);
+    if (lane == 0) {
+        s_a[warp] = a;
+        s_f[warp] = f;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 1; w < (T + 31) / 32; ++w) {
+            a += s_a[w];
+            f += s_f[w];
+        }
+        if (mode & kCloseMove) {
+            S->last_accepts = a;
+            S->total_accepts += a;
+            S->total_moves += (unsigned long long)S->n_beads;
+        }
+        if (mode & kCloseField) S->e_field = f;
+        if (mode & kCloseBond) {
+            S->e_bond = f;
+            S->e_bond_step = S->step + 1u;
+        }
+        if ((mode & kCloseAverage) && S->avg && S->avg_every && ((S->step + 1u) % S->avg_every) == 0u)
+            S->avg_samples += 1ull;
+        if (mode & kCloseFlip) S->cur ^= 1u;
+        if (mode & kCloseAdvance) S->step += 1u;
+    }
+    __syncthreads();
+}
+
 template <bool FUSED, int NT>
 __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ tiles, int n_tiles, int force_update,
-                                                double* __restrict__ ef_part) {
+                                                double* __restrict__ ef_part, int close_mode) {
     __shared__ double s_ef[32];
+    __shared__ unsigned long long s_acc[32];
     __shared__ float cf[kMaxTypes * kMaxTypes];
+    __shared__ int s_last;
     const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
         const FieldTile t = tiles[ti];
@@ -827,61 +875,38 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
             double e = 0.0;
             for (int w = 0; w < (T + 31) / 32; ++w) e += s_ef[w];
             ef_part[ti] = e;
+            if (close_mode) {
+                // publish the partial, then count the tile; the block that
+                // finishes a system's last tile closes it (no waiting)
+                __threadfence();
+                const unsigned done = atomicAdd(&S->field_done, 1u) + 1u;
+                s_last = done == (unsigned)t.n_tiles_sys;
+            }
+        }
+        __syncthreads();
+        if (close_mode && s_last) {
+            __threadfence();
+            close_system(S, ef_part + t.first_tile, t.n_tiles_sys, close_mode, s_acc, s_ef);
+            if (tid == 0) S->field_done = 0u;
         }
         __syncthreads();
     }
 }
 
-// Closes a launch for every system of the plan (one block per system): sums
-// the per-tile partials in a fixed order and updates the statistics, and for
-// a full sweep advances the step and makes the new counts current.
+// Closes a launch for every system of the plan (one block per system): the
+// sums of close_system over each system's tile ranges.
 __global__ void __launch_bounds__(256) k_close(const SysClose* __restrict__ list, int n_sys,
                                                 const unsigned* __restrict__ acc_part, int warps_per_tile,
                                                 const double* __restrict__ ef_part, const double* __restrict__ eb_part,
                                                 int mode) {
-    __shared__ unsigned long long s_a[256];
-    __shared__ double s_f[256];
-    const int tid = threadIdx.x, T = blockDim.x;
+    __shared__ unsigned long long s_a[32];
+    __shared__ double s_f[32];
     for (int si = blockIdx.x; si < n_sys; si += gridDim.x) {
         const SysClose L = list[si];
-        SysDev* S = L.sys;
-        unsigned long long a = 0;
-        double f = 0.0;
-        if ((mode & kCloseMove) && tid < kSlots) {
-            a = S->slot_acc[tid];
-            S->slot_acc[tid] = 0ull;
-        }
-        if (mode & kCloseField)
-            for (int i = tid; i < L.field_count; i += T) f += ef_part[L.field_first + i];
         if (mode & kCloseBond)
-            for (int i = tid; i < L.move_count; i += T) f += eb_part[L.move_first + i];
-        s_a[tid] = a;
-        s_f[tid] = f;
-        __syncthreads();
-        for (int o = T / 2; o > 0; o >>= 1) {
-            if (tid < o) {
-                s_a[tid] += s_a[tid + o];
-                s_f[tid] += s_f[tid + o];
-            }
-            __syncthreads();
-        }
-        if (tid == 0) {
-            if (mode & kCloseMove) {
-                S->last_accepts = s_a[0];
-                S->total_accepts += s_a[0];
-                S->total_moves += (unsigned long long)S->n_beads;
-            }
-            if (mode & kCloseField) S->e_field = s_f[0];
-            if (mode & kCloseBond) {
-                S->e_bond = s_f[0];
-                S->e_bond_step = S->step + 1u;
-            }
-            if ((mode & kCloseAverage) && S->avg && S->avg_every && ((S->step + 1u) % S->avg_every) == 0u)
-                S->avg_samples += 1ull;
-            if (mode & kCloseFlip) S->cur ^= 1u;
-            if (mode & kCloseAdvance) S->step += 1u;
-        }
-        __syncthreads();
+            close_system(L.sys, eb_part + L.move_first, L.move_count, mode, s_a, s_f);
+        else
+            close_system(L.sys, ef_part + L.field_first, L.field_count, mode, s_a, s_f);
     }
 }
 
@@ -1157,27 +1182,27 @@ int launch_sweep(int mode, const MoveTile* tiles, int n_tiles, int mtb, int ml, 
 
 template <bool FUSED>
 static void launch_field_t(int nt, const FieldTile* tiles, int n_tiles, int force_update, int blocks, int threads,
-                           double* ef, cudaStream_t st) {
+                           double* ef, int close_mode, cudaStream_t st) {
     if (nt == 2)
-        k_field<FUSED, 2><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef);
+        k_field<FUSED, 2><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef, close_mode);
     else if (nt == 3)
-        k_field<FUSED, 3><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef);
+        k_field<FUSED, 3><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef, close_mode);
     else if (nt == 1)
-        k_field<FUSED, 1><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef);
+        k_field<FUSED, 1><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef, close_mode);
     else
-        k_field<FUSED, 0><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef);
+        k_field<FUSED, 0><<<blocks, threads, 0, st>>>(tiles, n_tiles, force_update, ef, close_mode);
 }
 
 int launch_field(bool fused, int force_update, const FieldTile* tiles, int n_tiles, LaunchShape sh, double* ef_part,
-                 void* stream) {
+                 int close_mode, void* stream) {
     if (n_tiles <= 0) return 0;
     cudaStream_t st = (cudaStream_t)stream;
     const int blocks = sh.blocks > 0 ? sh.blocks : n_tiles;
     const int threads = sh.threads > 256 ? 256 : sh.threads;
     if (fused)
-        launch_field_t<true>(sh.n_types, tiles, n_tiles, force_update, blocks, threads, ef_part, st);
+        launch_field_t<true>(sh.n_types, tiles, n_tiles, force_update, blocks, threads, ef_part, close_mode, st);
     else
-        launch_field_t<false>(sh.n_types, tiles, n_tiles, force_update, blocks, threads, ef_part, st);
+        launch_field_t<false>(sh.n_types, tiles, n_tiles, force_update, blocks, threads, ef_part, close_mode, st);
     return (int)cudaGetLastError();
 }
 
