@@ -305,7 +305,9 @@ typedef struct scmf_tune {
     int32_t threads_field;     /* 0 = default */
     int32_t persistent_ctas;   /* 0 = one CTA per tile (no persistence) */
     int32_t use_graph;         /* 1 = capture one sweep in a CUDA graph */
-    int32_t reserved[2];
+    int32_t beads_per_tile;    /* > 0: chains per tile = max(1, beads_per_tile / length) for each
+                                  architecture (takes precedence over chains_per_tile) */
+    int32_t reserved;
 } scmf_tune;
 
 scmf_status scmf_batch_create(scmf_system* const* systems, int32_t n, const scmf_tune* tune,

@@ -47,7 +47,7 @@ class Stats(C.Structure):
 class Tune(C.Structure):
     _fields_ = [("chains_per_tile", C.c_int32), ("threads_move", C.c_int32), ("cells_per_tile", C.c_int32),
                 ("threads_field", C.c_int32), ("persistent_ctas", C.c_int32), ("use_graph", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("beads_per_tile", C.c_int32), ("reserved", C.c_int32)]
 
 
 class ServerOpts(C.Structure):

@@ -702,9 +702,6 @@ scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps, scmf_tune* out) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    int max_len = 1;
-    for (auto* s : b->systems)
-        for (auto& a : s->archs) max_len = std::max(max_len, a.length);
     auto trial = [&](const scmf_tune& t, float* ms) -> scmf_status {
         DevPlan dp;
         Plan p;
@@ -725,7 +722,7 @@ scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps, scmf_tune* out) {
     scmf_tune best = b->plan.tune;
     float best_ms = 1e30f;
     if (!rc) {
-        const int tile_beads[] = {512, 1024, 2048, 4096};
+        const int tile_beads[] = {1024, 2048, 4096, 8192};
         const int threads[] = {64, 128, 256};
         const int persist[] = {0, 148 * 4};
         for (int tb : tile_beads)
@@ -733,7 +730,8 @@ scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps, scmf_tune* out) {
                 for (int pc : persist) {
                     if (rc) break;
                     scmf_tune t = b->plan.tune;
-                    t.chains_per_tile = std::max(1, tb / max_len);
+                    t.chains_per_tile = 0;
+                    t.beads_per_tile = tb;
                     t.threads_move = th;
                     t.persistent_ctas = pc;
                     float ms = 0;

@@ -243,7 +243,7 @@ void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d) {
 scmf_tune default_tune() {
     scmf_tune t{};
     t.chains_per_tile = 0;
-    t.threads_move = 256;
+    t.threads_move = 128;  // 4 warps: CTAs retire and refill at a finer grain than 8-warp CTAs
     t.cells_per_tile = 0;
     t.threads_field = 256;
     t.persistent_ctas = 0;
@@ -260,6 +260,7 @@ scmf_tune resolve_tune(const scmf_tune* t) {
     if (t->threads_field > 0) r.threads_field = std::min(256, std::max(32, t->threads_field / 32 * 32));
     r.persistent_ctas = std::max(0, t->persistent_ctas);
     r.use_graph = t->use_graph;
+    r.beads_per_tile = std::max(0, std::min(t->beads_per_tile, kMaxTileBeads));
     return r;
 }
 
@@ -377,15 +378,17 @@ using namespace scmf;
 
 // Work tiles of this system appended to a plan.
 scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
-    const int64_t target_small = std::max<int64_t>(1, n_beads / (2 * 148));
+    // systems below ~2.4M beads: four tiles per SM (measured best over the 256-system mix
+    // against two and six per SM with 4-warp CTAs)
+    const int64_t target_small = std::max<int64_t>(1, n_beads / (4 * 148));
     const size_t first_tile = p->move.size();
     const size_t first_field = p->field.size();
     for (size_t a = 0; a < archs.size(); ++a) {
         const ArchHost& A = archs[a];
         if (A.n_chains == 0) continue;
-        int cpt = t.chains_per_tile;
+        int cpt = t.beads_per_tile > 0 ? std::max(1, t.beads_per_tile / A.length) : t.chains_per_tile;
         if (cpt <= 0) {
-            const int64_t target = std::min<int64_t>(2048, std::max<int64_t>(A.length, target_small));
+            const int64_t target = std::min<int64_t>(4096, std::max<int64_t>(A.length, target_small));
             cpt = (int)std::max<int64_t>(1, target / A.length);
         }
         cpt = std::max(1, std::min(cpt, kMaxTileBeads / A.length));

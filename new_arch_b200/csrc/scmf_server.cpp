@@ -99,6 +99,7 @@ void scmf_server::run() {
     const int per_round = opts.sweeps_per_round > 0 ? opts.sweeps_per_round : 25;
     scmf_tune tune = default_tune();
     tune.use_graph = opts.use_graph;
+    tune.beads_per_tile = 4096;  // the active systems fill the GPU together: full-size tiles for all
     for (;;) {
         // admission
         std::vector<Request> admit;
