@@ -327,10 +327,17 @@ def run_batched(nb, batched_mix, args, torch):
         x.close()
     plain = beads * K / (plain_ms / 1e3)
     batched = beads * K / (batched_ms / 1e3)
+
+    def move_launches(lengths):
+        # one register-kernel launch per tile kind: chains filling warps exactly, chains across warps
+        kinds = {32 % ((n + 1) // 2) != 0 for n in lengths}
+        return len(kinds)
+    per_sys = sum(1 + move_launches([a.length for a in sp.archs]) for sp in specs)
+    per_batch = 1 + move_launches([a.length for sp in specs for a in sp.archs])
     return {"workload": "256 diblock systems, edges {16..64}^3, N {16..64}, 100 sweeps each", "beads": beads,
             "sweeps": K, "plain_bead_moves_per_s": plain, "batched_bead_moves_per_s": batched,
-            "batched_over_plain": batched / plain, "tune": tune, "gpu_launches_batched": 2 * K,
-            "gpu_launches_plain": 2 * K * len(specs)}
+            "batched_over_plain": batched / plain, "tune": tune, "gpu_launches_batched": per_batch * K,
+            "gpu_launches_plain": per_sys * K}
 
 
 def run_served(nb, served_request, args):

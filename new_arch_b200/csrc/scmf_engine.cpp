@@ -268,8 +268,11 @@ scmf_tune resolve_tune(const scmf_tune* t) {
 void DevPlan::release() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graph_src) cudaGraphDestroy(graph_src);
-    void* ptrs[] = {d_move, d_field, d_close, d_acc, d_ef, d_eb};
+    void* ptrs[] = {d_move, d_field, d_close, d_acc, d_ef, d_eb, d_flat_list, d_warp_list};
     for (void* p : ptrs) dev_free(p, stream);
+    d_flat_list = nullptr;
+    d_warp_list = nullptr;
+    n_flat = n_warp = 0;
     graph = nullptr;
     graph_src = nullptr;
     d_move = nullptr;
@@ -293,14 +296,22 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t, cudaStream_t st) 
     max_chains = p.max_chains;
     linear = p.linear;
     n_sys = (int)p.close.size();
+    std::vector<int32_t> fl, wl;
+    for (size_t i = 0; i < p.move.size(); ++i) (p.tile_flat[i] ? fl : wl).push_back((int32_t)i);
+    n_flat = (int)fl.size();
+    n_warp = (int)wl.size();
     const size_t nm = std::max<size_t>(1, p.move.size()), nf = std::max<size_t>(1, p.field.size());
     scmf_status rc;
     if ((rc = dev_alloc((void**)&d_move, nm * sizeof(MoveTile), st)) ||
         (rc = dev_alloc((void**)&d_field, nf * sizeof(FieldTile), st)) ||
         (rc = dev_alloc((void**)&d_close, std::max<size_t>(1, p.close.size()) * sizeof(SysClose), st)) ||
         (rc = dev_alloc((void**)&d_acc, nm * kMaxWarps * sizeof(unsigned), st)) ||
-        (rc = dev_alloc((void**)&d_ef, nf * sizeof(double), st)) || (rc = dev_alloc((void**)&d_eb, nm * sizeof(double), st)))
+        (rc = dev_alloc((void**)&d_ef, nf * sizeof(double), st)) || (rc = dev_alloc((void**)&d_eb, nm * sizeof(double), st)) ||
+        (rc = dev_alloc((void**)&d_flat_list, std::max<size_t>(1, fl.size()) * sizeof(int32_t), st)) ||
+        (rc = dev_alloc((void**)&d_warp_list, std::max<size_t>(1, wl.size()) * sizeof(int32_t), st)))
         return rc;
+    if (!fl.empty()) CK(cudaMemcpyAsync(d_flat_list, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice, st));
+    if (!wl.empty()) CK(cudaMemcpyAsync(d_warp_list, wl.data(), wl.size() * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(d_acc, 0, nm * kMaxWarps * sizeof(unsigned), st));
     CK(cudaMemcpyAsync(d_move, p.move.data(), p.move.size() * sizeof(MoveTile), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(d_field, p.field.data(), p.field.size() * sizeof(FieldTile), cudaMemcpyHostToDevice, st));
@@ -317,6 +328,10 @@ LaunchShape DevPlan::move_shape() const {
     sh.n_types = n_types_uniform;
     sh.linear = linear ? 1 : 0;
     sh.max_chains = max_chains;
+    sh.flat_list = d_flat_list;
+    sh.n_flat = n_flat;
+    sh.warp_list = d_warp_list;
+    sh.n_warp = n_warp;
     return sh;
 }
 
@@ -402,6 +417,7 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
             mt.n_tiles_sys = 0;
             mt.arch_index = (int32_t)a;
             p->move.push_back(mt);
+            p->tile_flat.push_back(A.linear && A.length <= 64 && 32 % ((A.length + 1) / 2) != 0 ? 1 : 0);
             p->max_tile_beads = std::max(p->max_tile_beads, mt.n_chains * A.length);
             p->max_chains = std::max(p->max_chains, mt.n_chains);
         }

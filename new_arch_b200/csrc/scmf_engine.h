@@ -65,6 +65,7 @@ struct Plan {
     int max_deg = 0;
     int max_chains = 0;   // most chains in one move tile
     bool linear = true;
+    std::vector<uint8_t> tile_flat;  // per move tile: chains run across warps (32 % ceil(L/2) != 0)
 };
 
 struct DevPlan {
@@ -77,6 +78,9 @@ struct DevPlan {
     int n_move = 0, n_field = 0, n_sys = 0;
     int max_tile_beads = 0, max_length = 0, n_types_uniform = 0, max_chains = 0;
     bool linear = false;
+    int32_t* d_flat_list = nullptr;  // tile indices for the block-wide register kernel
+    int32_t* d_warp_list = nullptr;  // tile indices for the warp-wise register kernel
+    int n_flat = 0, n_warp = 0;
     scmf_tune tune{};
     cudaGraphExec_t graph = nullptr;
     cudaGraph_t graph_src = nullptr;

@@ -148,6 +148,13 @@ struct LaunchShape {
     int n_types;   // field kernel: monomer types shared by all systems, 0 = mixed
     int linear;    // sweep kernel: every architecture is a linear chain
     int max_chains;  // sweep kernel: most chains in one tile
+    // sweep kernel, linear chains of at most 64 beads: tiles whose ceil(L/2)
+    // does not divide 32 (chains laid across warps) and the others, as lists
+    // of tile indices; n_flat == 0 means every tile is a warp tile
+    const int32_t* flat_list;
+    int n_flat;
+    const int32_t* warp_list;
+    int n_warp;
 };
 
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);

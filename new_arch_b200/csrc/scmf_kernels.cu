@@ -362,14 +362,20 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
 #define SCMF_SWEEP_MIN_BLOCKS 4
 #endif
 template <int MODE>
-__global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(const MoveTile* __restrict__ tiles, int n_tiles,
+__global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(const MoveTile* __restrict__ tiles,
+                                                          const int32_t* __restrict__ list, int n_list,
                                                           int warp_beads, unsigned* __restrict__ acc_part) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    float* sx = reinterpret_cast<float*>(smem_raw) + (size_t)warp * 3 * warp_beads;
+    // per warp: x, y, z of its chains (parity-split), then the spare sine of
+    // every even bead's block, which its odd partner takes as first normal
+    const int spare_len = (warp_beads + 1) / 2;
+    float* sx = reinterpret_cast<float*>(smem_raw) + (size_t)warp * (3 * warp_beads + spare_len);
     float* sy = sx + warp_beads;
     float* sz = sy + warp_beads;
-    for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
+    float* ssp = sz + warp_beads;
+    for (int li = blockIdx.x; li < n_list; li += gridDim.x) {
+        const int ti = list ? __ldg(list + li) : li;
         const MoveTile t = tiles[ti];
         SysDev* S = t.sys;
         const ArchDev* Ap = t.arch;
@@ -453,7 +459,15 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
                     }
                     const int type = __ldg(types + b);
                     float n0, n1, n2;
-                    const uint32_t aw = bead_normals(gc, b, step, k0, k1, n0, n1, n2);
+                    const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1);
+                    if (col == 0) {
+                        float sp;
+                        normals3_spare(w, n0, n1, n2, sp);
+                        ssp[cl * h0 + k] = sp;                  // for odd bead b + 1
+                    } else {
+                        normals3_odd(ssp[cl * h0 + k], w, n0, n1, n2);  // spare of even bead b - 1
+                    }
+                    const uint32_t aw = accept_word(w);
                     float px, py, pz;
                     int cell;
                     const bool acc = trial<2>(c, sx[me], sy[me], sz[me], qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
@@ -504,28 +518,39 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
 }
 
 // Linear chains of at most 64 beads, positions in registers.  Each thread owns
-// the bead pair (2t, 2t+1) of one chain (ceil(L/2) threads per chain, as many
-// chains per warp as fit).  Even half-sweep: bead 2t moves against 2t-1 (the
-// odd bead of lane-1, by shuffle) and 2t+1 (its own); odd half-sweep: bead
-// 2t+1 moves against 2t (its own, already moved) and 2t+2 (the even bead of
-// lane+1).  No shared memory, no block barrier; tiles are read and written
-// with coalesced float2 accesses.  Same trial and keys as k_sweep.
+// the bead pair (2t, 2t+1) of one chain (ceil(L/2) threads per chain).  Even
+// half-sweep: bead 2t moves against 2t-1 (the odd bead of lane-1, by shuffle)
+// and 2t+1 (its own); odd half-sweep: bead 2t+1 moves against 2t (its own,
+// already moved) and 2t+2 (the even bead of lane+1).  When ceil(L/2) divides
+// 32, each warp holds whole chains: no shared memory, no block barrier.
+// Otherwise (L = 48: 24 threads per chain would idle a quarter of every warp)
+// the block holds as many whole chains as fit in all its threads, chains run
+// across warp boundaries, and the two boundary neighbours go through shared
+// memory between two block barriers per iteration; every chain still moves
+// all its even beads before any odd bead.  Tiles are read and written with
+// coalesced float2 accesses.  Same trial and keys as k_sweep.
 #ifndef SCMF_REG_MIN_BLOCKS
 #define SCMF_REG_MIN_BLOCKS 3
 #endif
-template <int MODE>
-__global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const MoveTile* __restrict__ tiles, int n_tiles,
+template <int MODE, bool ANY_FLAT>
+__global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const MoveTile* __restrict__ tiles,
+                                                                        const int32_t* __restrict__ list, int n_list,
                                                                         unsigned* __restrict__ acc_part) {
+    __shared__ float s_last_odd[kMaxWarps][3];    // odd bead of each warp's lane 31, before the move
+    __shared__ float s_first_even[kMaxWarps][3];  // even bead of each warp's lane 0, after the move
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
+    for (int li = blockIdx.x; li < n_list; li += gridDim.x) {
+        const int ti = list ? __ldg(list + li) : li;  // tile index in the plan
         const MoveTile t = tiles[ti];
         SysDev* S = t.sys;
         const ArchDev* Ap = t.arch;
         const int L = Ap->length;
         const int tpc = (L + 1) >> 1;                        // threads per chain
-        const int cpw = 32 / tpc;                            // chains per warp
-        const int cs = (int)div_magic((uint32_t)lane, Ap->tpc_magic, tpc);
-        const int tt = lane - cs * tpc;                      // pair index in the chain
+        const bool flat = ANY_FLAT && (32 % tpc) != 0;       // chains run across warps (block-uniform)
+        const int slot = flat ? (int)threadIdx.x : lane;     // pair slot in the block / in the warp
+        const int cpw = flat ? (int)blockDim.x / tpc : 32 / tpc;  // chains per block / per warp iteration
+        const int cs = (int)div_magic((uint32_t)slot, Ap->tpc_magic, tpc);
+        const int tt = slot - cs * tpc;                      // pair index in the chain
         const int be = 2 * tt, bo = 2 * tt + 1;
         MoveConsts c;
         c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
@@ -543,7 +568,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
         const int type_o = cs < cpw && bo < L ? __ldg(Ap->types + bo) : 0;
         const bool pair_aligned = ((t.bead0 & 1) == 0) && ((L & 1) == 0);
         unsigned nacc = 0;
-        for (int cbase = warp * cpw; cbase < t.n_chains; cbase += nwarps * cpw) {
+        for (int cbase = flat ? 0 : warp * cpw; cbase < t.n_chains; cbase += flat ? cpw : nwarps * cpw) {
             const int chain = cbase + cs;
             const bool live = cs < cpw && chain < t.n_chains;
             const bool has_o = live && bo < L;
@@ -584,9 +609,18 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
             float spare = 0.0f;  // spare sine of the even bead's block, first normal of the odd bead
             // even half-sweep
             {
-                const float lx = __shfl_up_sync(0xffffffffu, xo, 1);
-                const float ly = __shfl_up_sync(0xffffffffu, yo, 1);
-                const float lz = __shfl_up_sync(0xffffffffu, zo, 1);
+                float lx = __shfl_up_sync(0xffffffffu, xo, 1);
+                float ly = __shfl_up_sync(0xffffffffu, yo, 1);
+                float lz = __shfl_up_sync(0xffffffffu, zo, 1);
+                if (flat) {
+                    if (lane == 31) {
+                        s_last_odd[warp][0] = xo; s_last_odd[warp][1] = yo; s_last_odd[warp][2] = zo;
+                    }
+                    __syncthreads();
+                    if (lane == 0 && warp > 0) {
+                        lx = s_last_odd[warp - 1][0]; ly = s_last_odd[warp - 1][1]; lz = s_last_odd[warp - 1][2];
+                    }
+                }
                 if (live) {
                     float qx[2], qy[2], qz[2];
                     int deg = 0;
@@ -610,9 +644,18 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
             }
             // odd half-sweep
             {
-                const float rx = __shfl_down_sync(0xffffffffu, xe, 1);
-                const float ry = __shfl_down_sync(0xffffffffu, ye, 1);
-                const float rz = __shfl_down_sync(0xffffffffu, ze, 1);
+                float rx = __shfl_down_sync(0xffffffffu, xe, 1);
+                float ry = __shfl_down_sync(0xffffffffu, ye, 1);
+                float rz = __shfl_down_sync(0xffffffffu, ze, 1);
+                if (flat) {
+                    if (lane == 0) {
+                        s_first_even[warp][0] = xe; s_first_even[warp][1] = ye; s_first_even[warp][2] = ze;
+                    }
+                    __syncthreads();
+                    if (lane == 31 && warp + 1 < nwarps) {
+                        rx = s_first_even[warp + 1][0]; ry = s_first_even[warp + 1][1]; rz = s_first_even[warp + 1][2];
+                    }
+                }
                 if (has_o) {
                     float qx[2], qy[2], qz[2];
                     qx[0] = xe; qy[0] = ye; qz[0] = ze;
@@ -1156,14 +1199,23 @@ static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, L
     if (mtb > kMaxTileBeads || ml > kMaxLength || sh.threads > 256 || sh.threads < 32) return (int)cudaErrorInvalidValue;
     const int blocks = sh.blocks > 0 ? sh.blocks : n_tiles;
     if (sh.linear && ml <= 64) {
-        k_sweep_reg<MODE><<<blocks, sh.threads, 0, st>>>(tiles, n_tiles, acc);
+        // tiles whose chains fill warps exactly run the barrier-free kernel,
+        // the others (sh.flat_list) the block-wide one: one launch each
+        const int n_warp = sh.n_flat > 0 ? sh.n_warp : n_tiles;
+        const int32_t* warp_list = sh.n_flat > 0 ? sh.warp_list : nullptr;
+        if (n_warp > 0)
+            k_sweep_reg<MODE, false><<<sh.blocks > 0 ? min(sh.blocks, n_warp) : n_warp, sh.threads, 0, st>>>(
+                tiles, warp_list, n_warp, acc);
+        if (sh.n_flat > 0)
+            k_sweep_reg<MODE, true><<<sh.blocks > 0 ? min(sh.blocks, sh.n_flat) : sh.n_flat, sh.threads, 0, st>>>(
+                tiles, sh.flat_list, sh.n_flat, acc);
     } else if (sh.linear) {
         // per-warp slice: ceil(chains per tile / warps) chains of the longest length
         const int nw = sh.threads / 32;
         const int wb = ((sh.max_chains + nw - 1) / nw) * ml;
-        const size_t smem = (size_t)nw * 3 * wb * sizeof(float);
+        const size_t smem = (size_t)nw * (3 * wb + (wb + 1) / 2) * sizeof(float);
         if (smem > sweep_smem_bytes(kMaxTileBeads, kMaxLength)) return (int)cudaErrorInvalidValue;
-        k_sweep_linear<MODE><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, wb, acc);
+        k_sweep_linear<MODE><<<blocks, sh.threads, smem, st>>>(tiles, nullptr, n_tiles, wb, acc);
     } else {
         const size_t smem = sweep_smem_bytes(mtb, ml);
         k_sweep<MODE, false><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml, acc);

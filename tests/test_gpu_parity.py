@@ -86,6 +86,58 @@ def test_blend_mixed_lengths(nb):
         compare_state(s, orc, "blend")
 
 
+@pytest.mark.parametrize("threads", [64, 128, 256])
+def test_chains_across_warps(nb, threads):
+    """Lengths whose ceil(L/2) does not divide 32 (48, 40, 24, 6, 5) run with
+    chains laid across warp boundaries; in one batch beside lengths that fill
+    warps exactly (32, 16), every system equals the oracle bit for bit."""
+    from new_arch_b200.spec import diblock_melt
+    lengths = (48, 40, 24, 6, 5, 32, 16)
+    specs = [diblock_melt(max(3, int(7.8 * 6 * 6 * 5 / n)), n, 0.4, (6, 6, 5), 18.0, 50.0, seed=70 + n)
+             for n in lengths]
+    systems = [nb.System(sp) for sp in specs]
+    for x in systems:
+        x.init_coords()
+    b = nb.Batch(systems, tune={"beads_per_tile": 1024, "threads_move": threads})
+    b.step(4)
+    for n, sp, x in zip(lengths, specs, systems):
+        orc = oracle_for(sp)
+        orc.step(4)
+        compare_state(x, orc, f"L={n} threads={threads}")
+    b.close()
+    for x in systems:
+        x.close()
+
+
+@pytest.mark.parametrize("lengths", [(80,), (65, 100), (48, 96, 16)])
+def test_long_linear_chains(nb, lengths):
+    """Chains longer than 64 beads take the shared-memory kernel (which keeps
+    each even bead's spare sine for its odd partner); every length in the
+    system goes through it, against the oracle bit for bit."""
+    from new_arch_b200.spec import SystemSpec, cell_units, diblock_arch, interaction_matrix
+    k, sig = cell_units()
+    archs = [diblock_arch(n, 0.5, max(2, int(7.8 * 8 * 8 * 6 / n / len(lengths))), sig) for n in lengths]
+    spec = SystemSpec(2, 8, 8, 6, 8.0, 8.0, 6.0, interaction_matrix(2, 20.0, 50.0), 64, k, 0.5, 91,
+                      nb.HAM_SCMF0, nb.FIELD_EVERY, 32, archs)
+    with nb.System(spec) as s:
+        s.init_coords()
+        orc = oracle_for(spec)
+        s.step(5)
+        orc.step(5)
+        compare_state(s, orc, f"lengths {lengths}")
+
+
+def test_chains_across_warps_alone(nb):
+    from new_arch_b200.spec import diblock_melt
+    spec = diblock_melt(700, 48, 0.3, (12, 10, 8), 25.0, 50.0, seed=48)
+    with nb.System(spec) as s:
+        s.init_coords()
+        orc = oracle_for(spec)
+        s.step(5)
+        orc.step(5)
+        compare_state(s, orc, "L=48 alone")
+
+
 def test_branched_three_types_literal_field(nb):
     """A comb with side chains (greedy colouring), three monomer types, the
     literal field and 16-bit counts."""
