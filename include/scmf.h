@@ -43,6 +43,7 @@ typedef int32_t scmf_status;
 #define SCMF_E_STATE (-6)     /* call not allowed in the current state */
 #define SCMF_E_TIMEOUT (-7)   /* a bounded wait ran out */
 #define SCMF_E_DEVICE (-8)    /* a kernel reported an error word */
+#define SCMF_E_CANCELLED (-9) /* a served request was cancelled before it finished */
 
 #define SCMF_MAX_TYPES 8      /* monomer types */
 #define SCMF_MAX_DEGREE 8     /* bonds per bead */
@@ -267,6 +268,27 @@ scmf_status scmf_checkpoint_info(const char* path, scmf_checkpoint_header* out);
 /* spec_hash a checkpoint of systems of this spec carries. */
 scmf_status scmf_spec_hash(const scmf_spec* spec, uint64_t* out);
 
+/* ------------------------------------------------------------- validation
+ * The reference has no sanitizer or checks (bounds printf()s and one trap,
+ * device_function.cu:159-160, 490-502, 610, 646-651).  scmf_validate checks
+ * the state on the device and reports instead of trapping: non-finite
+ * positions, positions beyond the exact range of the FP32 cell fold
+ * (|x / dx| >= 2^22 on some axis; the cell index stays in range but is no
+ * longer the floor), count words differing from a fresh gridding of the
+ * positions (counts are stale between scmf_smc_move and
+ * scmf_reset_density_fields), per-type counts not summing to that type's
+ * beads, and non-finite omega.  Returns SCMF_E_DEVICE when any is nonzero. */
+typedef struct scmf_validation {
+    uint64_t nonfinite_positions;
+    uint64_t positions_out_of_range;
+    uint64_t count_mismatch_words;   /* 32-bit words of the counts array (16-bit counts come in pairs) */
+    uint64_t nonfinite_omega;
+    int64_t count_sum_error;         /* sum over types of |sum of counts - beads of the type| */
+    uint32_t error_word;             /* the kernels' error word */
+    uint32_t reserved;
+} scmf_validation;
+scmf_status scmf_validate(scmf_system* sys, scmf_validation* out);
+
 /* --------------------------------------------------------------- analysis
  * Chain observables as device reductions (double), per architecture: the
  * reference's end-to-end distance (test.cpp:47-68, beads 0 and 31 of every
@@ -340,12 +362,14 @@ typedef struct scmf_server_opts {
 
 typedef struct scmf_result {
     uint64_t id;
-    scmf_status status;
-    int32_t n_sweeps;
+    scmf_status status;         /* SCMF_OK, SCMF_E_CANCELLED, or the error that ended the request */
+    int32_t n_sweeps;           /* requested */
     double e_bond, e_field;
     uint64_t accepts;
     int64_t n_beads;
-    double t_submit, t_admit, t_done;   /* seconds on the server's monotonic clock */
+    double t_submit, t_admit, t_done;   /* seconds on the server's monotonic clock (t_admit 0: never admitted) */
+    int32_t sweeps_done;
+    int32_t reserved;
 } scmf_result;
 
 scmf_status scmf_server_create(const scmf_server_opts* opts, scmf_server** out);
@@ -356,6 +380,14 @@ scmf_status scmf_server_submit(scmf_server* s, const scmf_spec* spec, int32_t n_
 /* Up to max results; waits up to wait_ms for at least one. */
 scmf_status scmf_server_poll(scmf_server* s, scmf_result* out, int32_t max, int32_t* n_out, int32_t wait_ms);
 scmf_status scmf_server_pending(scmf_server* s, int32_t* queued, int32_t* active, uint64_t* bytes_in_use);
+/* Cancels a request: a queued one leaves the queue at once, an active one at
+ * the next round boundary (its device memory is freed); either way one result
+ * with status SCMF_E_CANCELLED and the sweeps done so far is delivered.
+ * SCMF_E_INVALID if the id is unknown or its result is already delivered. */
+scmf_status scmf_server_cancel(scmf_server* s, uint64_t id);
+/* Waits until no request is queued or active: SCMF_OK, or SCMF_E_TIMEOUT
+ * after timeout_ms (the requests keep running). */
+scmf_status scmf_server_drain(scmf_server* s, int32_t timeout_ms);
 double scmf_server_now(const scmf_server* s);
 void scmf_server_destroy(scmf_server* s);
 

@@ -12,7 +12,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libscmf.so")
 
 SCMF_OK = 0
-ERRORS = {-1: "INVALID", -2: "CUDA", -3: "NOMEM", -4: "IO", -5: "PARSE", -6: "STATE", -7: "TIMEOUT", -8: "DEVICE"}
+ERRORS = {-1: "INVALID", -2: "CUDA", -3: "NOMEM", -4: "IO", -5: "PARSE", -6: "STATE", -7: "TIMEOUT", -8: "DEVICE",
+          -9: "CANCELLED"}
 
 HAM_SCMF0, HAM_LITERAL = 0, 1
 FIELD_REFERENCE, FIELD_EVERY = 0, 1
@@ -58,7 +59,8 @@ class ServerOpts(C.Structure):
 class Result(C.Structure):
     _fields_ = [("id", C.c_uint64), ("status", C.c_int32), ("n_sweeps", C.c_int32), ("e_bond", C.c_double),
                 ("e_field", C.c_double), ("accepts", C.c_uint64), ("n_beads", C.c_int64),
-                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+                ("sweeps_done", C.c_int32), ("reserved", C.c_int32)]
 
 
 class CheckpointHeader(C.Structure):
@@ -74,6 +76,12 @@ class Observables(C.Structure):
     _fields_ = [("arch", C.c_int32), ("n_chains", C.c_int32), ("n_beads", C.c_int64), ("n_bonds", C.c_int64),
                 ("re2", C.c_double * 4), ("rg2", C.c_double * 4), ("bond2", C.c_double * 4), ("msd", C.c_double * 4),
                 ("msd_com", C.c_double * 4), ("acc_ratio", C.c_double), ("reserved", C.c_double * 3)]
+
+
+class Validation(C.Structure):
+    _fields_ = [("nonfinite_positions", C.c_uint64), ("positions_out_of_range", C.c_uint64),
+                ("count_mismatch_words", C.c_uint64), ("nonfinite_omega", C.c_uint64),
+                ("count_sum_error", C.c_int64), ("error_word", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 # name -> (restype, argtypes)
@@ -132,6 +140,7 @@ SIGNATURES = {
     "scmf_checkpoint_read": (_i32, [_vp, C.c_char_p]),
     "scmf_checkpoint_info": (_i32, [C.c_char_p, C.POINTER(CheckpointHeader)]),
     "scmf_spec_hash": (_i32, [_vp, C.POINTER(C.c_uint64)]),
+    "scmf_validate": (_i32, [_vp, C.POINTER(Validation)]),
     "scmf_analysis_reference": (_i32, [_vp]),
     "scmf_analyze": (_i32, [_vp, C.POINTER(Observables), _i32]),
     "scmf_batch_create": (_i32, [_pvp, _i32, C.POINTER(Tune), _vp, _pvp]),
@@ -146,6 +155,8 @@ SIGNATURES = {
     "scmf_server_poll": (_i32, [_vp, C.POINTER(Result), _i32, _pi32, _i32]),
     "scmf_server_pending": (_i32, [_vp, _pi32, _pi32, C.POINTER(C.c_uint64)]),
     "scmf_server_now": (_f64, [_vp]),
+    "scmf_server_cancel": (_i32, [_vp, _u64]),
+    "scmf_server_drain": (_i32, [_vp, _i32]),
     "scmf_server_destroy": (None, [_vp]),
 }
 

@@ -44,7 +44,7 @@ void free_system(scmf_system* s) {
     if (!s) return;
     s->plan.release();
     void* ptrs[] = {s->x, s->y, s->z, s->chain_id, s->counts[0], s->counts[1], s->omega, s->d_sys, s->d_arch,
-                    s->d_arch_blob, s->d_aos, s->d_u32, s->d_avg, s->d_ref, s->d_obs};
+                    s->d_arch_blob, s->d_aos, s->d_u32, s->d_avg, s->d_ref, s->d_obs, s->d_check};
     for (void* p : ptrs) dev_free(p, s->stream);
     if (s->own_stream && s->stream) {
         cudaStreamSynchronize(s->stream);

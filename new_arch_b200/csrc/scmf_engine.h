@@ -124,6 +124,7 @@ struct scmf_system {
     unsigned long long* d_avg = nullptr;  // time-averaged density accumulator (while averaging)
     float* d_ref = nullptr;      // reference snapshot for displacements, SoA (lazy)
     double* d_obs = nullptr;     // per-tile observable partials (lazy)
+    unsigned long long* d_check = nullptr;  // validation counters (lazy)
     std::vector<scmf::ArchHost> archs;
     std::vector<scmf::ArchDev> h_arch;  // host image of d_arch
     scmf::DevPlan plan;                  // default work plan of this system alone

@@ -175,6 +175,12 @@ int launch_aos_to_soa(const float* aos, SysDev* sys, const ArchDev* arch, int n_
 int launch_soa_to_aos(float* aos, const SysDev* sys, const ArchDev* arch, int n_arch, int64_t n_beads,
                       void* stream);
 int launch_unpack_counts16(const SysDev* sys, uint32_t* out, int64_t n, void* stream);
+// Validation (scmf_validate): out[0] += non-finite positions, out[1] +=
+// positions beyond the exact fold range; out[2] += differing count words of
+// a and b, out[3] += non-finite omega; sums[t] += counts of type t.
+int launch_validate_positions(const SysDev* sys, int64_t n_beads, unsigned long long* out, void* stream);
+int launch_validate_cells(const SysDev* sys, const uint32_t* a, const uint32_t* b, int64_t n_words,
+                          int64_t n_values, unsigned long long* out, unsigned long long* sums, void* stream);
 // Adds the current counts into SysDev::avg and counts one sample.
 int launch_average_sample(SysDev* sys, int64_t n, void* stream);
 // Chain observables: kObsSlots partial sums per move tile into part; ref_xyz

@@ -1089,6 +1089,52 @@ __global__ void __launch_bounds__(256) k_observables(const MoveTile* __restrict_
     }
 }
 
+// State checks of scmf_validate (counters in out[], no trap).
+__global__ void k_validate_positions(const SysDev* S, int64_t n, unsigned long long* out) {
+    unsigned long long bad = 0, far = 0;
+    const float lim = 0x1p22f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float x = S->x[i], y = S->y[i], z = S->z[i];
+        if (!isfinite(x) || !isfinite(y) || !isfinite(z)) {
+            ++bad;
+            continue;
+        }
+        if (fabsf(x * S->inv_dx) >= lim || fabsf(y * S->inv_dy) >= lim || fabsf(z * S->inv_dz) >= lim) ++far;
+    }
+    bad = warp_sum(bad);
+    far = warp_sum(far);
+    if ((threadIdx.x & 31) == 0 && (bad | far)) {
+        atomicAdd(out + 0, bad);
+        atomicAdd(out + 1, far);
+    }
+}
+
+__global__ void k_validate_cells(const SysDev* S, const uint32_t* a, const uint32_t* b, int64_t n_words,
+                                 int64_t n_values, unsigned long long* out, unsigned long long* sums) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    unsigned long long diff = 0, bad = 0;
+    for (int64_t i = i0; i < n_words; i += stride) diff += a[i] != b[i] ? 1ull : 0ull;
+    for (int64_t i = i0; i < n_values; i += stride)
+        if (!isfinite(S->omega[i])) ++bad;
+    const bool c16 = S->count16 != 0;
+    const uint16_t* a16 = reinterpret_cast<const uint16_t*>(a);
+    const int64_t nc = S->n_cells;
+    for (int t = 0; t < S->n_types; ++t) {
+        unsigned long long v = 0;
+        for (int64_t c = i0; c < nc; c += stride)
+            v += c16 ? (unsigned long long)a16[t * nc + c] : (unsigned long long)a[t * nc + c];
+        v = warp_sum(v);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(sums + t, v);
+    }
+    diff = warp_sum(diff);
+    bad = warp_sum(bad);
+    if ((threadIdx.x & 31) == 0 && (diff | bad)) {
+        atomicAdd(out + 2, diff);
+        atomicAdd(out + 3, bad);
+    }
+}
+
 // ------------------------------------------------------------- transposes
 __device__ __forceinline__ int64_t aos_bead_of(const SysDev* S, const ArchDev* archs, int n_arch, int64_t i) {
     int a = 0;
@@ -1287,6 +1333,18 @@ int launch_soa_to_aos(float* aos, const SysDev* sys, const ArchDev* arch, int n_
 int launch_unpack_counts16(const SysDev* sys, uint32_t* out, int64_t n, void* stream) {
     if (n <= 0) return 0;
     k_unpack16<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(sys, out, n);
+    return (int)cudaGetLastError();
+}
+int launch_validate_positions(const SysDev* sys, int64_t n, unsigned long long* out, void* stream) {
+    if (n <= 0) return 0;
+    k_validate_positions<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(sys, n, out);
+    return (int)cudaGetLastError();
+}
+int launch_validate_cells(const SysDev* sys, const uint32_t* a, const uint32_t* b, int64_t n_words, int64_t n_values,
+                          unsigned long long* out, unsigned long long* sums, void* stream) {
+    const int64_t n = n_words > n_values ? n_words : n_values;
+    if (n <= 0) return 0;
+    k_validate_cells<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(sys, a, b, n_words, n_values, out, sums);
     return (int)cudaGetLastError();
 }
 int launch_average_sample(SysDev* sys, int64_t n, void* stream) {

@@ -12,6 +12,7 @@
 // No reference counterpart: the reference runs one system per process.
 #include <algorithm>
 #include <chrono>
+#include <unordered_set>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -51,6 +52,8 @@ struct scmf_server {
     std::deque<Request> queue;
     std::vector<Active> active;
     std::deque<scmf_result> done;
+    std::unordered_set<uint64_t> running;    // ids admitted and not yet finished
+    std::unordered_set<uint64_t> cancelled;  // running ids to drop at the next round boundary
     uint64_t next_id = 1;
     size_t bytes_in_use = 0;
     int n_active = 0;  // mirror of active.size() for other threads
@@ -70,6 +73,7 @@ static void finish(scmf_server* s, Active& a, scmf_status st) {
     r.id = a.req.id;
     r.status = st;
     r.n_sweeps = a.req.n_sweeps;
+    r.sweeps_done = a.req.n_sweeps - std::max(0, a.remaining);
     r.n_beads = a.sys ? a.sys->n_beads : 0;
     r.t_submit = a.req.t_submit;
     r.t_admit = a.t_admit;
@@ -88,6 +92,8 @@ static void finish(scmf_server* s, Active& a, scmf_status st) {
     r.t_done = s->now();
     std::lock_guard<std::mutex> g(s->mu);
     s->bytes_in_use -= std::min(s->bytes_in_use, a.req.bytes);
+    s->running.erase(r.id);
+    s->cancelled.erase(r.id);
     s->done.push_back(r);
     s->cv_done.notify_all();
 }
@@ -113,6 +119,7 @@ void scmf_server::run() {
                 const bool slot = opts.max_active <= 0 || (int)(active.size() + admit.size()) < opts.max_active;
                 if (!slot || bytes_in_use + r.bytes > opts.hbm_budget_bytes) break;
                 bytes_in_use += r.bytes;
+                running.insert(r.id);
                 admit.push_back(std::move(r));
                 queue.pop_front();
             }
@@ -134,6 +141,28 @@ void scmf_server::run() {
         {
             std::lock_guard<std::mutex> g(mu);
             n_active = (int)active.size();
+        }
+        // cancellations of running requests take effect at the round boundary
+        {
+            std::vector<uint64_t> drop;
+            {
+                std::lock_guard<std::mutex> g(mu);
+                for (auto& a : active)
+                    if (cancelled.count(a.req.id)) drop.push_back(a.req.id);
+            }
+            if (!drop.empty()) {
+                std::vector<Active> keep;
+                for (auto& a : active) {
+                    if (std::find(drop.begin(), drop.end(), a.req.id) != drop.end())
+                        finish(this, a, SCMF_E_CANCELLED);
+                    else
+                        keep.push_back(std::move(a));
+                }
+                active.swap(keep);
+                plan_valid = false;
+                std::lock_guard<std::mutex> g(mu);
+                n_active = (int)active.size();
+            }
         }
         if (active.empty()) continue;
         // one round over all active systems
@@ -235,6 +264,41 @@ scmf_status scmf_server_pending(scmf_server* s, int32_t* queued, int32_t* active
     if (queued) *queued = (int32_t)s->queue.size();
     if (active) *active = (int32_t)s->n_active;
     if (bytes) *bytes = s->bytes_in_use;
+    return SCMF_OK;
+}
+
+scmf_status scmf_server_cancel(scmf_server* s, uint64_t id) {
+    if (!s) return fail(SCMF_E_INVALID, "NULL server");
+    std::lock_guard<std::mutex> g(s->mu);
+    for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
+        if (it->id != id) continue;
+        scmf_result r{};
+        r.id = id;
+        r.status = SCMF_E_CANCELLED;
+        r.n_sweeps = it->n_sweeps;
+        r.t_submit = it->t_submit;
+        r.t_done = s->now();
+        s->queue.erase(it);
+        s->done.push_back(r);
+        s->cv_done.notify_all();
+        return SCMF_OK;
+    }
+    if (s->running.count(id)) {
+        s->cancelled.insert(id);
+        s->cv_work.notify_all();
+        return SCMF_OK;
+    }
+    return fail(SCMF_E_INVALID, "no queued or running request %llu", (unsigned long long)id);
+}
+
+scmf_status scmf_server_drain(scmf_server* s, int32_t timeout_ms) {
+    if (!s || timeout_ms < 0) return fail(SCMF_E_INVALID, "bad arguments");
+    std::unique_lock<std::mutex> lk(s->mu);
+    const bool idle = s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms),
+                                          [s] { return s->queue.empty() && s->running.empty(); });
+    if (!idle)
+        return fail(SCMF_E_TIMEOUT, "%zu queued and %zu running requests after %d ms", s->queue.size(),
+                    s->running.size(), (int)timeout_ms);
     return SCMF_OK;
 }
 

@@ -335,6 +335,59 @@ scmf_status scmf_checkpoint_read(scmf_system* s, const char* path) {
     return check_error_word(s);
 }
 
+// ------------------------------------------------------------- validation
+scmf_status scmf_validate(scmf_system* s, scmf_validation* out) {
+    if (!s || !out) return fail(SCMF_E_INVALID, "NULL argument");
+    std::memset(out, 0, sizeof *out);
+    constexpr int kCounters = 4;
+    if (!s->d_check)
+        RET(alloc_scratch((void**)&s->d_check, (kCounters + kMaxTypes) * sizeof(unsigned long long), s->stream));
+    CK(cudaMemsetAsync(s->d_check, 0, (kCounters + kMaxTypes) * sizeof(unsigned long long), s->stream));
+    SysDev d;
+    RET(fetch_sysdev(s, &d));
+    const uint32_t cur = d.cur & 1u;
+    const size_t cb = counts_bytes(s);
+    // a fresh gridding of the positions into the idle counts buffer (zero
+    // between calls), compared word by word with the current counts; the idle
+    // buffer is cleared again afterwards
+    const uint32_t other = cur ^ 1u;
+    CK(cudaMemsetAsync(s->counts[other], 0, cb, s->stream));
+    CK(cudaMemcpyAsync((char*)s->d_sys + offsetof(SysDev, cur), &other, 4, cudaMemcpyHostToDevice, s->stream));
+    LaunchShape sh = s->plan.move_shape();
+    sh.blocks = 0;
+    CKL(launch_sweep(kGridOnly, s->plan.d_move, s->plan.n_move, s->plan.max_tile_beads, s->plan.max_length, sh,
+                     s->plan.d_acc, s->stream));
+    CK(cudaMemcpyAsync((char*)s->d_sys + offsetof(SysDev, cur), &cur, 4, cudaMemcpyHostToDevice, s->stream));
+    CKL(launch_validate_positions(s->d_sys, s->n_beads, s->d_check, s->stream));
+    CKL(launch_validate_cells(s->d_sys, s->counts[cur], s->counts[other], (int64_t)(cb / 4),
+                              (int64_t)cells_total(s), s->d_check, s->d_check + kCounters, s->stream));
+    CK(cudaMemsetAsync(s->counts[other], 0, cb, s->stream));
+    unsigned long long h[kCounters + kMaxTypes];
+    CK(cudaMemcpyAsync(h, s->d_check, sizeof h, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    out->nonfinite_positions = h[0];
+    out->positions_out_of_range = h[1];
+    out->count_mismatch_words = h[2];
+    out->nonfinite_omega = h[3];
+    std::vector<int64_t> per_type(s->spec.n_types, 0);
+    for (const auto& a : s->archs)
+        for (const auto& b : a.beads) per_type[b.type] += a.n_chains;
+    int64_t err = 0;
+    for (int t = 0; t < s->spec.n_types; ++t) err += std::llabs((int64_t)h[kCounters + t] - per_type[t]);
+    out->count_sum_error = err;
+    RET(fetch_sysdev(s, &d));
+    out->error_word = d.error_word;
+    if (out->nonfinite_positions || out->positions_out_of_range || out->count_mismatch_words ||
+        out->nonfinite_omega || out->count_sum_error || out->error_word)
+        return fail(SCMF_E_DEVICE,
+                    "state check: %llu non-finite positions, %llu beyond the fold range, %llu count words differ "
+                    "from the positions, %llu non-finite omega, count sum error %lld, error word 0x%x",
+                    (unsigned long long)out->nonfinite_positions, (unsigned long long)out->positions_out_of_range,
+                    (unsigned long long)out->count_mismatch_words, (unsigned long long)out->nonfinite_omega,
+                    (long long)out->count_sum_error, out->error_word);
+    return SCMF_OK;
+}
+
 // --------------------------------------------------------------- analysis
 scmf_status scmf_analysis_reference(scmf_system* s) {
     if (!s) return fail(SCMF_E_INVALID, "NULL system");

@@ -40,7 +40,7 @@ class Server:
         out = []
         for i in range(n.value):
             r = arr[i]
-            d = {k: getattr(r, k) for k, _ in _lib.Result._fields_}
+            d = {k: getattr(r, k) for k, _ in _lib.Result._fields_ if k != "reserved"}
             d["counts"] = self._buffers.pop(r.id, None)
             out.append(d)
         return out
@@ -52,6 +52,14 @@ class Server:
 
     def now(self) -> float:
         return lib().scmf_server_now(self._h)
+
+    def cancel(self, rid: int) -> None:
+        """Cancel a queued or running request; its result arrives with status -9."""
+        check(lib().scmf_server_cancel(self._h, int(rid)))
+
+    def drain(self, timeout_ms: int) -> None:
+        """Wait until nothing is queued or running; ScmfError(-7) on timeout."""
+        check(lib().scmf_server_drain(self._h, int(timeout_ms)))
 
     def close(self) -> None:
         h = getattr(self, "_h", None)

@@ -172,6 +172,18 @@ class System:
     def checkpoint_read(self, path: str) -> None:
         check(lib().scmf_checkpoint_read(self._h, path.encode()))
 
+    # -------------------------------------------------------- validation
+    def validate(self, raise_on_error: bool = True) -> dict:
+        """Device-side state checks (finite and in-range positions, counts equal
+        to a fresh gridding and conserved per type, finite omega)."""
+        v = _lib.Validation()
+        rc = lib().scmf_validate(self._h, C.byref(v))
+        if raise_on_error:
+            check(rc)
+        d = {k: getattr(v, k) for k, _ in _lib.Validation._fields_ if k != "reserved"}
+        d["ok"] = rc == 0
+        return d
+
     # ---------------------------------------------------------- analysis
     def analysis_reference(self) -> None:
         """Current positions become the origin of the displacements."""

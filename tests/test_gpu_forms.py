@@ -212,3 +212,38 @@ def test_cli_checkpoint_resume_and_average(nb, tmp_path):
     # the end-to-end line is the device reduction of the same positions
     line_a = [l for l in r.stdout.splitlines() if l.startswith("step 20 end")]
     assert line_a
+
+
+def test_server_cancel_and_drain(nb):
+    """A cancelled queued request never runs; a cancelled running one stops at
+    a round boundary with its sweeps so far; the others finish as if alone;
+    a drain with a tiny limit times out while work remains, then succeeds."""
+    from new_arch_b200.server import Server
+    from new_arch_b200.spec import diblock_melt
+    sp = diblock_melt(3000, 16, 0.5, (16, 16, 16), 20.0, 50.0, seed=8)
+    budget = int(sp.device_bytes() * 2.5)             # two systems at a time
+    K = 5000
+    with Server(budget, sweeps_per_round=2) as srv:
+        ids = [srv.submit(sp, K) for _ in range(4)]
+        srv.cancel(ids[3])                             # still queued: the budget holds two
+        t0 = time.time()
+        while srv.pending()[1] < 1 and time.time() - t0 < 30:
+            time.sleep(0.001)
+        srv.cancel(ids[0])                             # admitted first, so running now
+        with pytest.raises(nb.ScmfError) as e:
+            srv.drain(1)
+        assert e.value.code == -7
+        with pytest.raises(nb.ScmfError) as e:
+            srv.cancel(12345)
+        assert e.value.code == -1
+        srv.drain(120_000)
+        res = {r["id"]: r for r in srv.poll(16, 1000)}
+    assert sorted(res) == sorted(ids)
+    assert res[ids[3]]["status"] == -9 and res[ids[3]]["sweeps_done"] == 0 and res[ids[3]]["t_admit"] == 0
+    assert res[ids[0]]["status"] == -9 and 0 <= res[ids[0]]["sweeps_done"] < K and res[ids[0]]["t_admit"] > 0
+    cnt, st = _alone(nb, sp, K)
+    for i in ids[1:3]:
+        r = res[i]
+        assert r["status"] == 0 and r["sweeps_done"] == K
+        assert_counts_equal(r["counts"], cnt, "served counts after cancellations")
+        assert r["accepts"] == st["total_accepts"]

@@ -148,3 +148,49 @@ def test_observables_match_oracle(nb):
             np.testing.assert_allclose(g[k][:3], o[k], rtol=1e-9, err_msg=f"arch {ai} {k}")
             assert abs(g[k][3] - g[k][:3].sum()) <= 1e-12 * abs(g[k][3])
         assert g["acc_ratio"] == st["last_accepts"] / spec.n_beads
+
+
+# ------------------------------------------------------------ validation
+def test_validate_clean_and_stale_counts(nb):
+    from new_arch_b200.spec import diblock_melt
+    for bits, grid in ((32, (8, 8, 8)), (16, (6, 5, 4))):
+        spec = diblock_melt(int(7.8 * np.prod(grid) / 16), 16, 0.4, grid, 20.0, 50.0, seed=2, count_bits=bits)
+        with nb.System(spec) as s:
+            s.init_coords()
+            s.step(3)
+            v = s.validate()
+            assert v["ok"] and v["count_mismatch_words"] == 0 and v["count_sum_error"] == 0
+            s.smc_move(1)                       # counts now lag the positions
+            v = s.validate(raise_on_error=False)
+            assert not v["ok"] and v["count_mismatch_words"] > 0 and v["count_sum_error"] == 0
+            s.reset_density_fields()
+            assert s.validate()["ok"]
+            s.step(2)                           # validation left the idle counts buffer clear
+            orc = oracle_for(spec)
+            orc.step(3)
+            orc.smc_move(1)
+            orc.reset_density()
+            orc.step(2)
+            compare_state(s, orc, f"after validation ({bits}-bit counts)")
+
+
+def test_validate_reports_bad_positions(nb):
+    """Host-made bad input: one non-finite coordinate and one far outside the
+    exact fold range.  The fold keeps every cell index inside the grid, so the
+    state stays usable; the check reports both beads and nothing else."""
+    from new_arch_b200.spec import diblock_melt
+    for grid in ((8, 8, 8), (6, 5, 7)):
+        spec = diblock_melt(40, 16, 0.5, grid, 20.0, 50.0, seed=3)
+        with nb.System(spec) as s:
+            s.init_coords()
+            xyz = s.coords().copy()
+            xyz[5, 1] = np.nan
+            xyz[17, 2] = 3.0e8
+            s.set_coords(xyz)
+            v = s.validate(raise_on_error=False)
+            assert not v["ok"]
+            assert v["nonfinite_positions"] == 1 and v["positions_out_of_range"] == 1
+            assert v["count_sum_error"] == 0 and v["count_mismatch_words"] == 0
+            with pytest.raises(nb.ScmfError) as e:
+                s.validate()
+            assert e.value.code == -8
