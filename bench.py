@@ -267,7 +267,7 @@ def run_ours(args):
             "clocks": clocks, "e2e": e2e, "gpu_launches": 2 * args.steps,
             "accept_ratio": accept_ratio,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": peak_kind, "kernel": "k_sweep<move+grid>",
+                         "peak_source": peak_kind, "kernel": "k_sweep_reg<move+grid>",
                          "alg_bytes_per_launch": alg_bytes,
                          "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
                          "ms_per_launch": ms_move / args.steps},
