@@ -268,6 +268,14 @@ scmf_tune resolve_tune(const scmf_tune* t) {
 void DevPlan::release() {
     if (graph) cudaGraphExecDestroy(graph);
     if (graph_src) cudaGraphDestroy(graph_src);
+    if (side) {
+        cudaStreamSynchronize(side);
+        cudaStreamDestroy(side);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    side = nullptr;
+    ev_fork = ev_join = nullptr;
     void* ptrs[] = {d_move, d_field, d_close, d_acc, d_ef, d_eb, d_flat_list, d_warp_list};
     for (void* p : ptrs) dev_free(p, stream);
     d_flat_list = nullptr;
@@ -300,6 +308,11 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t, cudaStream_t st) 
     for (size_t i = 0; i < p.move.size(); ++i) (p.tile_flat[i] ? fl : wl).push_back((int32_t)i);
     n_flat = (int)fl.size();
     n_warp = (int)wl.size();
+    if (n_flat > 0 && n_warp > 0 && p.linear && p.max_length <= 64) {
+        CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    }
     const size_t nm = std::max<size_t>(1, p.move.size()), nf = std::max<size_t>(1, p.field.size());
     scmf_status rc;
     if ((rc = dev_alloc((void**)&d_move, nm * sizeof(MoveTile), st)) ||
@@ -350,7 +363,19 @@ scmf_status DevPlan::enqueue_close(int mode, cudaStream_t st) const {
 }
 
 scmf_status DevPlan::enqueue_sweep(cudaStream_t st) const {
-    CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, move_shape(), d_acc, st));
+    if (side && n_warp > 0 && n_flat > 0) {
+        LaunchShape warp = move_shape(), flat = move_shape();
+        warp.part = 1;
+        flat.part = 2;
+        CK(cudaEventRecord(ev_fork, st));
+        CK(cudaStreamWaitEvent(side, ev_fork, 0));
+        CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, flat, d_acc, side));
+        CK(cudaEventRecord(ev_join, side));
+        CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, warp, d_acc, st));
+        CK(cudaStreamWaitEvent(st, ev_join, 0));
+    } else {
+        CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, move_shape(), d_acc, st));
+    }
     CKL(launch_field(true, 0, d_field, n_field, field_shape(), d_ef, kSweepClose, st));
     return SCMF_OK;
 }

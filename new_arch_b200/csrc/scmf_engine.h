@@ -85,6 +85,11 @@ struct DevPlan {
     cudaGraphExec_t graph = nullptr;
     cudaGraph_t graph_src = nullptr;
     cudaStream_t stream = nullptr;  // allocations of the plan are ordered on it
+    // plans with both warp-wise and flat tiles run the two move launches side
+    // by side (fork on ev_fork, join on ev_join) so neither waits for the
+    // other's last partial wave
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     void release();
     scmf_status upload(const Plan& p, const scmf_tune& t, cudaStream_t st);
     LaunchShape move_shape() const;

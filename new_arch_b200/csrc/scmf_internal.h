@@ -155,6 +155,7 @@ struct LaunchShape {
     int n_flat;
     const int32_t* warp_list;
     int n_warp;
+    int part;        // 0: every tile; 1: warp tiles only; 2: flat tiles only
 };
 
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);

@@ -1249,10 +1249,10 @@ static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, L
         // the others (sh.flat_list) the block-wide one: one launch each
         const int n_warp = sh.n_flat > 0 ? sh.n_warp : n_tiles;
         const int32_t* warp_list = sh.n_flat > 0 ? sh.warp_list : nullptr;
-        if (n_warp > 0)
+        if (n_warp > 0 && sh.part != 2)
             k_sweep_reg<MODE, false><<<sh.blocks > 0 ? min(sh.blocks, n_warp) : n_warp, sh.threads, 0, st>>>(
                 tiles, warp_list, n_warp, acc);
-        if (sh.n_flat > 0)
+        if (sh.n_flat > 0 && sh.part != 1)
             k_sweep_reg<MODE, true><<<sh.blocks > 0 ? min(sh.blocks, sh.n_flat) : sh.n_flat, sh.threads, 0, st>>>(
                 tiles, sh.flat_list, sh.n_flat, acc);
     } else if (sh.linear) {
