@@ -93,6 +93,13 @@ scmf_status ensure_aos(scmf_system* s) {
     return dalloc(&s->d_aos, (size_t)s->n_beads * 3 * sizeof(float), &dummy, s->stream);
 }
 
+scmf_status set_stop_step(scmf_system* s, uint32_t stop_step) {
+    CK(cudaMemcpyAsync((char*)s->d_sys + offsetof(SysDev, stop_step), &stop_step, 4, cudaMemcpyHostToDevice,
+                       s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return SCMF_OK;
+}
+
 scmf_status check_error_word(const scmf_system* s) {
     SysDev d;
     RET(fetch_sysdev(s, &d));

@@ -213,6 +213,7 @@ void field_coefficients(int n, const double* xn, int nref, int hamiltonian, floa
 }
 
 void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d) {
+    d->stop_step = 0xFFFFFFFFu;
     d->n_types = s.n_types;
     d->nx = s.nx; d->ny = s.ny; d->nz = s.nz;
     d->n_cells = (int64_t)s.nx * s.ny * s.nz;

@@ -155,4 +155,6 @@ scmf_status regrid(scmf_system* s);         // counts of the current positions i
 scmf_status field_now(scmf_system* s);      // omega of the current counts (always updated)
 scmf_status ensure_aos(scmf_system* s);     // AoS staging buffer
 scmf_status check_error_word(const scmf_system* s);
+// Fused sweeps skip the system once its step reaches stop_step (served form).
+scmf_status set_stop_step(scmf_system* s, uint32_t stop_step);
 }  // namespace scmf

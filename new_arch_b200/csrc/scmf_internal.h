@@ -90,6 +90,11 @@ struct SysDev {
     unsigned long long avg_samples;  // sweeps accumulated
     uint32_t avg_every;
     uint32_t field_done;  // field tiles of the running launch finished (the last one closes the sweep)
+    // fused sweeps leave the system alone once step reaches stop_step (the
+    // served form gives each request its own sweep count inside a shared
+    // round); 0xFFFFFFFF everywhere else
+    uint32_t stop_step;
+    uint32_t pad3;
 };
 
 // Work item of the move / grid kernel: a run of whole chains of one architecture.

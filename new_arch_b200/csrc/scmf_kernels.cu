@@ -191,6 +191,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
     for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
         const MoveTile t = tiles[ti];
         SysDev* S = t.sys;
+        if (MODE != kGridOnly && S->step >= S->stop_step) continue;  // block-uniform
         const ArchDev* Ap = t.arch;
         const int L = Ap->length;
         const int nb = t.n_chains * L;
@@ -378,6 +379,7 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
         const int ti = list ? __ldg(list + li) : li;
         const MoveTile t = tiles[ti];
         SysDev* S = t.sys;
+        if (MODE != kGridOnly && S->step >= S->stop_step) continue;
         const ArchDev* Ap = t.arch;
         const int L = Ap->length;
         const int h0 = (L + 1) >> 1;
@@ -543,6 +545,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
         const int ti = list ? __ldg(list + li) : li;  // tile index in the plan
         const MoveTile t = tiles[ti];
         SysDev* S = t.sys;
+        if (MODE != kGridOnly && S->step >= S->stop_step) continue;  // block-uniform
         const ArchDev* Ap = t.arch;
         const int L = Ap->length;
         const int tpc = (L + 1) >> 1;                        // threads per chain
@@ -887,6 +890,7 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
     for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
         const FieldTile t = tiles[ti];
         SysDev* S = t.sys;
+        if (FUSED && S->step >= S->stop_step) continue;  // block-uniform: the system's sweeps are done
         for (int i = tid; i < kMaxTypes * kMaxTypes; i += T) cf[i] = S->cf[i];
         __syncthreads();
         const uint32_t cur = S->cur;

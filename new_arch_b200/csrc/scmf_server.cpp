@@ -1,23 +1,32 @@
 // Served form of the engine: a request loop with continuous batching.
 //
 // Requests (a system spec + a sweep count) are queued by scmf_server_submit.
-// One worker thread owns the GPU work: between rounds it admits queued
-// requests in arrival order while their device memory fits the HBM budget
-// (and the active-slot limit), creates and initialises their systems, then
-// runs one round of sweeps over every active system with the batched plan
-// (one move launch and one field launch per sweep for all of them).  Systems
-// stay resident between rounds; a system whose sweeps are done is read back
-// (counts, energies) and freed, and its memory goes to the next request.
-// Requests that arrive while others run join at the next round boundary.
-// No reference counterpart: the reference runs one system per process.
+// Three threads keep the GPU busy:
+//   admission   takes queued requests in arrival order while their device
+//               memory fits the HBM budget (and the slot limit), creates each
+//               system on its own stream, initialises it there (random walks,
+//               grid, field) and marks it ready; this runs beside the rounds.
+//   rounds      at each round boundary adds the ready systems, drops the
+//               finished and cancelled ones, rebuilds the batched plan if the
+//               set changed, and runs a fixed number of sweeps over every
+//               active system on the server stream (one move and one field
+//               launch per sweep for all of them).  A system stops at its own
+//               sweep count inside the round: its SysDev stop_step makes the
+//               kernels skip its tiles, so rounds are not cut short by the
+//               request with the fewest sweeps left.
+//   completion  reads finished systems back (energies, accepts, counts) on
+//               their own streams and frees them while the next round runs.
+// Systems stay resident between rounds; requests that arrive while others run
+// join at the next round boundary.  No reference counterpart: the reference
+// runs one system per process.
 #include <algorithm>
 #include <chrono>
-#include <unordered_set>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <mutex>
 #include <thread>
+#include <unordered_set>
 #include <vector>
 
 #include "scmf_engine.h"
@@ -40,6 +49,7 @@ struct Active {
     scmf_system* sys = nullptr;
     int remaining = 0;
     double t_admit = 0;
+    scmf_status status = SCMF_OK;  // status to report when it reaches completion
 };
 
 }  // namespace
@@ -48,36 +58,48 @@ struct scmf_server {
     scmf_server_opts opts{};
     int device = 0;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work;   // admission: queue changed or stop
+    std::condition_variable cv_ready;  // rounds: a system is ready or stop
+    std::condition_variable cv_fin;    // completion: a system finished or stop
+    std::condition_variable cv_done;   // clients: a result was delivered
     std::deque<Request> queue;
-    std::vector<Active> active;
+    std::deque<Active> ready;          // initialised, waiting for the next round boundary
+    std::deque<Active> finishing;      // handed to the completion thread
     std::deque<scmf_result> done;
-    std::unordered_set<uint64_t> running;    // ids admitted and not yet finished
-    std::unordered_set<uint64_t> cancelled;  // running ids to drop at the next round boundary
+    std::unordered_set<uint64_t> running;    // admitted and not yet delivered
+    std::unordered_set<uint64_t> cancelled;  // running ids to drop
     uint64_t next_id = 1;
     size_t bytes_in_use = 0;
-    int n_active = 0;  // mirror of active.size() for other threads
-    bool stop = false;
-    std::thread worker;
-    cudaStream_t stream = nullptr;
+    int n_active = 0;  // systems in the current rounds (mirror for other threads)
+    bool stop = false, admission_done = false, rounds_done = false;
+    std::thread admitter, worker, completer;
+    cudaStream_t stream = nullptr;  // the rounds' stream
     std::chrono::steady_clock::time_point t0;
 
     double now() const {
         return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
-    void run();
+    void admit_loop();
+    void round_loop();
+    void complete_loop();
+    void hand_over(Active&& a) {
+        std::lock_guard<std::mutex> g(mu);
+        finishing.push_back(std::move(a));
+        cv_fin.notify_all();
+    }
 };
 
-static void finish(scmf_server* s, Active& a, scmf_status st) {
+// Reads a finished system back into its result and frees it (completion thread).
+static void finish(scmf_server* s, Active& a) {
     scmf_result r{};
     r.id = a.req.id;
-    r.status = st;
+    r.status = a.status;
     r.n_sweeps = a.req.n_sweeps;
     r.sweeps_done = a.req.n_sweeps - std::max(0, a.remaining);
     r.n_beads = a.sys ? a.sys->n_beads : 0;
     r.t_submit = a.req.t_submit;
     r.t_admit = a.t_admit;
-    if (a.sys && st == SCMF_OK) {
+    if (a.sys && a.status == SCMF_OK) {
         scmf_stats stats{};
         scmf_status rc = scmf_get_stats(a.sys, &stats);
         if (!rc && a.req.counts_out)
@@ -98,7 +120,56 @@ static void finish(scmf_server* s, Active& a, scmf_status st) {
     s->cv_done.notify_all();
 }
 
-void scmf_server::run() {
+void scmf_server::admit_loop() {
+    cudaSetDevice(device);
+    for (;;) {
+        Request r;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            for (;;) {
+                if (stop && queue.empty()) {
+                    admission_done = true;
+                    cv_ready.notify_all();
+                    return;
+                }
+                if (!queue.empty()) {
+                    const Request& q = queue.front();
+                    const bool slot = opts.max_active <= 0 || (int)running.size() < opts.max_active;
+                    if (slot && bytes_in_use + q.bytes <= opts.hbm_budget_bytes) break;
+                }
+                // wait for a submission, a freed slot or memory, or shutdown
+                cv_work.wait_for(lk, std::chrono::milliseconds(50));
+            }
+            r = std::move(queue.front());
+            queue.pop_front();
+            bytes_in_use += r.bytes;
+            running.insert(r.id);
+        }
+        Active a;
+        a.req = std::move(r);
+        a.remaining = a.req.n_sweeps;
+        a.t_admit = now();
+        // a private stream: creation and initialisation overlap the rounds
+        scmf_status rc = scmf_system_create(&a.req.spec, nullptr, &a.sys);
+        if (!rc) rc = scmf_init_coords(a.sys);
+        if (!rc) rc = set_stop_step(a.sys, (uint32_t)a.req.n_sweeps);
+        bool drop;
+        {
+            std::lock_guard<std::mutex> g(mu);
+            drop = cancelled.count(a.req.id) > 0;
+        }
+        if (rc || drop || a.remaining == 0) {
+            a.status = rc ? rc : (drop ? SCMF_E_CANCELLED : SCMF_OK);
+            hand_over(std::move(a));
+            continue;
+        }
+        std::lock_guard<std::mutex> g(mu);
+        ready.push_back(std::move(a));
+        cv_ready.notify_all();
+    }
+}
+
+void scmf_server::round_loop() {
     cudaSetDevice(device);
     DevPlan plan;
     bool plan_valid = false;
@@ -106,96 +177,88 @@ void scmf_server::run() {
     scmf_tune tune = default_tune();
     tune.use_graph = opts.use_graph;
     tune.beads_per_tile = 4096;  // the active systems fill the GPU together: full-size tiles for all
+    std::vector<Active> active;
     for (;;) {
-        // admission
-        std::vector<Request> admit;
+        // round boundary: take ready systems, drop cancelled ones
+        std::vector<uint64_t> drop;
         {
             std::unique_lock<std::mutex> lk(mu);
-            if (active.empty() && queue.empty() && !stop)
-                cv_work.wait_for(lk, std::chrono::milliseconds(50));
-            if (stop && queue.empty() && active.empty()) break;
-            while (!queue.empty()) {
-                Request& r = queue.front();
-                const bool slot = opts.max_active <= 0 || (int)(active.size() + admit.size()) < opts.max_active;
-                if (!slot || bytes_in_use + r.bytes > opts.hbm_budget_bytes) break;
-                bytes_in_use += r.bytes;
-                running.insert(r.id);
-                admit.push_back(std::move(r));
-                queue.pop_front();
+            if (active.empty() && ready.empty()) {
+                if (admission_done) break;
+                cv_ready.wait_for(lk, std::chrono::milliseconds(50));
             }
+            while (!ready.empty()) {
+                active.push_back(std::move(ready.front()));
+                ready.pop_front();
+                plan_valid = false;
+            }
+            for (auto& a : active)
+                if (cancelled.count(a.req.id)) drop.push_back(a.req.id);
         }
-        for (auto& r : admit) {
-            Active a;
-            a.req = std::move(r);
-            a.remaining = a.req.n_sweeps;
-            a.t_admit = now();
-            scmf_status rc = scmf_system_create(&a.req.spec, stream, &a.sys);
-            if (!rc) rc = scmf_init_coords(a.sys);
-            if (rc || a.remaining == 0) {
-                finish(this, a, rc);
-                continue;
+        if (!drop.empty()) {
+            std::vector<Active> keep;
+            for (auto& a : active) {
+                if (std::find(drop.begin(), drop.end(), a.req.id) != drop.end()) {
+                    a.status = SCMF_E_CANCELLED;
+                    hand_over(std::move(a));
+                } else {
+                    keep.push_back(std::move(a));
+                }
             }
-            active.push_back(std::move(a));
+            active.swap(keep);
             plan_valid = false;
         }
         {
             std::lock_guard<std::mutex> g(mu);
             n_active = (int)active.size();
         }
-        // cancellations of running requests take effect at the round boundary
-        {
-            std::vector<uint64_t> drop;
-            {
-                std::lock_guard<std::mutex> g(mu);
-                for (auto& a : active)
-                    if (cancelled.count(a.req.id)) drop.push_back(a.req.id);
-            }
-            if (!drop.empty()) {
-                std::vector<Active> keep;
-                for (auto& a : active) {
-                    if (std::find(drop.begin(), drop.end(), a.req.id) != drop.end())
-                        finish(this, a, SCMF_E_CANCELLED);
-                    else
-                        keep.push_back(std::move(a));
-                }
-                active.swap(keep);
-                plan_valid = false;
-                std::lock_guard<std::mutex> g(mu);
-                n_active = (int)active.size();
-            }
-        }
         if (active.empty()) continue;
-        // one round over all active systems
-        int round = per_round;
-        for (auto& a : active) round = std::min(round, a.remaining);
+        int round = 0;
+        for (auto& a : active) round = std::max(round, std::min(per_round, a.remaining));
+        scmf_status rc = SCMF_OK;
         if (!plan_valid) {
             Plan p;
             for (auto& a : active) a.sys->append_plan(tune, &p);
-            scmf_status rc = plan.upload(p, tune, stream);
-            if (rc) {
-                for (auto& a : active) finish(this, a, rc);
-                active.clear();
-                continue;
-            }
-            plan_valid = true;
+            rc = plan.upload(p, tune, stream);
+            plan_valid = rc == SCMF_OK;
         }
-        scmf_status rc = plan.run_sweeps(stream, round);
+        if (!rc) rc = plan.run_sweeps(stream, round);
         if (!rc && cudaStreamSynchronize(stream) != cudaSuccess) rc = fail(SCMF_E_CUDA, "round failed");
         std::vector<Active> keep;
         for (auto& a : active) {
-            a.remaining -= round;
-            if (rc || a.remaining <= 0) {
-                finish(this, a, rc);
+            a.remaining = std::max(0, a.remaining - round);
+            if (rc || a.remaining == 0) {
+                a.status = rc;
+                hand_over(std::move(a));
                 plan_valid = false;
             } else {
                 keep.push_back(std::move(a));
             }
         }
         active.swap(keep);
-        std::lock_guard<std::mutex> g(mu);
-        n_active = (int)active.size();
     }
     plan.release();
+    std::lock_guard<std::mutex> g(mu);
+    n_active = 0;
+    rounds_done = true;
+    cv_fin.notify_all();
+}
+
+void scmf_server::complete_loop() {
+    cudaSetDevice(device);
+    for (;;) {
+        Active a;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_fin.wait(lk, [this] { return !finishing.empty() || (rounds_done && admission_done); });
+            if (finishing.empty()) return;
+            a = std::move(finishing.front());
+            finishing.pop_front();
+        }
+        finish(this, a);
+        std::lock_guard<std::mutex> g(mu);
+        cv_work.notify_all();  // memory and a slot came free
+    }
 }
 
 extern "C" {
@@ -216,7 +279,9 @@ scmf_status scmf_server_create(const scmf_server_opts* opts, scmf_server** out) 
         delete s;
         return fail(SCMF_E_CUDA, "cudaStreamCreate failed");
     }
-    s->worker = std::thread([s] { s->run(); });
+    s->admitter = std::thread([s] { s->admit_loop(); });
+    s->worker = std::thread([s] { s->round_loop(); });
+    s->completer = std::thread([s] { s->complete_loop(); });
     *out = s;
     return SCMF_OK;
 }
@@ -285,7 +350,6 @@ scmf_status scmf_server_cancel(scmf_server* s, uint64_t id) {
     }
     if (s->running.count(id)) {
         s->cancelled.insert(id);
-        s->cv_work.notify_all();
         return SCMF_OK;
     }
     return fail(SCMF_E_INVALID, "no queued or running request %llu", (unsigned long long)id);
@@ -310,8 +374,12 @@ void scmf_server_destroy(scmf_server* s) {
         std::lock_guard<std::mutex> g(s->mu);
         s->stop = true;
         s->cv_work.notify_all();
+        s->cv_ready.notify_all();
+        s->cv_fin.notify_all();
     }
+    if (s->admitter.joinable()) s->admitter.join();
     if (s->worker.joinable()) s->worker.join();
+    if (s->completer.joinable()) s->completer.join();
     cudaStreamDestroy(s->stream);
     delete s;
 }
