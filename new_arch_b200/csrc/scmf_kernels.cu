@@ -527,9 +527,10 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
 // 32, each warp holds whole chains: no shared memory, no block barrier.
 // Otherwise (L = 48: 24 threads per chain would idle a quarter of every warp)
 // the block holds as many whole chains as fit in all its threads, chains run
-// across warp boundaries, and the two boundary neighbours go through shared
-// memory between two block barriers per iteration; every chain still moves
-// all its even beads before any odd bead.  Tiles are read and written with
+// across warp boundaries: a warp's first even bead reads its left neighbour
+// from global memory (not yet moved, not yet stored), its last odd bead gets
+// the moved right neighbour through shared memory after one block barrier per
+// iteration; every chain still moves all its even beads before any odd bead.  Tiles are read and written with
 // coalesced float2 accesses.  Same trial and keys as k_sweep.
 #ifndef SCMF_REG_MIN_BLOCKS
 #define SCMF_REG_MIN_BLOCKS 3
@@ -538,8 +539,11 @@ template <int MODE, bool ANY_FLAT>
 __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const MoveTile* __restrict__ tiles,
                                                                         const int32_t* __restrict__ list, int n_list,
                                                                         unsigned* __restrict__ acc_part) {
-    __shared__ float s_last_odd[kMaxWarps][3];    // odd bead of each warp's lane 31, before the move
-    __shared__ float s_first_even[kMaxWarps][3];  // even bead of each warp's lane 0, after the move
+    // even bead of each warp's lane 0 after its move, double-buffered by
+    // iteration parity: with one barrier per iteration a warp may write the
+    // next iteration's slot while its left neighbour still reads this one
+    __shared__ float s_first_even[2][kMaxWarps][3];
+    int parity = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int li = blockIdx.x; li < n_list; li += gridDim.x) {
         const int ti = list ? __ldg(list + li) : li;  // tile index in the plan
@@ -615,14 +619,13 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                 float lx = __shfl_up_sync(0xffffffffu, xo, 1);
                 float ly = __shfl_up_sync(0xffffffffu, yo, 1);
                 float lz = __shfl_up_sync(0xffffffffu, zo, 1);
-                if (flat) {
-                    if (lane == 31) {
-                        s_last_odd[warp][0] = xo; s_last_odd[warp][1] = yo; s_last_odd[warp][2] = zo;
-                    }
-                    __syncthreads();
-                    if (lane == 0 && warp > 0) {
-                        lx = s_last_odd[warp - 1][0]; ly = s_last_odd[warp - 1][1]; lz = s_last_odd[warp - 1][2];
-                    }
+                if (flat && lane == 0 && warp > 0 && live && tt > 0) {
+                    // the previous warp's last odd bead, not yet moved: positions of this
+                    // iteration are stored only after the barrier below, so global memory
+                    // still holds its start-of-sweep value (read through L2)
+                    lx = __ldcg(S->x + g - 1);
+                    ly = __ldcg(S->y + g - 1);
+                    lz = __ldcg(S->z + g - 1);
                 }
                 if (live) {
                     float qx[2], qy[2], qz[2];
@@ -652,12 +655,17 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                 float rz = __shfl_down_sync(0xffffffffu, ze, 1);
                 if (flat) {
                     if (lane == 0) {
-                        s_first_even[warp][0] = xe; s_first_even[warp][1] = ye; s_first_even[warp][2] = ze;
+                        s_first_even[parity][warp][0] = xe;
+                        s_first_even[parity][warp][1] = ye;
+                        s_first_even[parity][warp][2] = ze;
                     }
                     __syncthreads();
                     if (lane == 31 && warp + 1 < nwarps) {
-                        rx = s_first_even[warp + 1][0]; ry = s_first_even[warp + 1][1]; rz = s_first_even[warp + 1][2];
+                        rx = s_first_even[parity][warp + 1][0];
+                        ry = s_first_even[parity][warp + 1][1];
+                        rz = s_first_even[parity][warp + 1][2];
                     }
+                    parity ^= 1;
                 }
                 if (has_o) {
                     float qx[2], qy[2], qz[2];
