@@ -53,6 +53,7 @@ scmf_status prepare_archs(const scmf_spec& s, std::vector<ArchHost>* out, int64_
 uint32_t magic_for(uint32_t n);
 size_t system_device_bytes(const scmf_spec& s);
 void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d);
+int fold_kind_of(const scmf_spec& s);  // 0: every grid axis a power of two, 1: otherwise
 
 // Work decomposition of one or many systems for one launch shape.
 struct Plan {
@@ -65,6 +66,7 @@ struct Plan {
     int max_deg = 0;
     int max_chains = 0;   // most chains in one move tile
     bool linear = true;
+    int fold_kind = 0;  // largest fold_kind_of() of the systems
     std::vector<uint8_t> tile_flat;  // per move tile: chains run across warps (32 % ceil(L/2) != 0)
 };
 
@@ -81,6 +83,7 @@ struct DevPlan {
     int32_t* d_flat_list = nullptr;  // tile indices for the block-wide register kernel
     int32_t* d_warp_list = nullptr;  // tile indices for the warp-wise register kernel
     int n_flat = 0, n_warp = 0;
+    int fold_kind = 0;
     scmf_tune tune{};
     cudaGraphExec_t graph = nullptr;
     cudaGraph_t graph_src = nullptr;

@@ -94,7 +94,6 @@ struct SysDev {
     // served form gives each request its own sweep count inside a shared
     // round); 0xFFFFFFFF everywhere else
     uint32_t stop_step;
-    uint32_t pad3;
 };
 
 // Work item of the move / grid kernel: a run of whole chains of one architecture.
@@ -161,6 +160,7 @@ struct LaunchShape {
     const int32_t* warp_list;
     int n_warp;
     int part;        // 0: every tile; 1: warp tiles only; 2: flat tiles only
+    int fold;        // 0: every system's grid axes are powers of two (mask-only fold)
 };
 
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);

@@ -74,12 +74,22 @@ __global__ void k_init_coords(SysDev* __restrict__ S, const ArchDev* __restrict_
 struct MoveConsts {
     float k, k2, A, R, inv_dx, inv_dy, inv_dz;
     int nx, ny, nz;
-    bool pow2;  // nx, ny, nz all powers of two
+    bool pow2;  // every axis a power of two
 };
 
+__device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
+
+__device__ __forceinline__ void load_fold(MoveConsts& c, const SysDev* S) {
+    c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
+    c.pow2 = is_pow2(c.nx) && is_pow2(c.ny) && is_pow2(c.nz);
+}
+
+// FOLD = 0: every system of the launch has power-of-two axes, so only the
+// mask fold is compiled in; FOLD = -1 picks the fold per system at run time.
+template <int FOLD = -1>
 __device__ __forceinline__ int cell_of(const MoveConsts& c, float x, float y, float z) {
     int ix, iy, iz;
-    if (c.pow2) {
+    if (FOLD == 0 || c.pow2) {
         ix = fold_pow2(x, c.inv_dx, c.nx - 1);
         iy = fold_pow2(y, c.inv_dy, c.ny - 1);
         iz = fold_pow2(z, c.inv_dz, c.nz - 1);
@@ -91,7 +101,6 @@ __device__ __forceinline__ int cell_of(const MoveConsts& c, float x, float y, fl
     return ix + c.nx * (iy + c.ny * iz);
 }
 
-__device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
 
 // One smart-MC trial (device_function.cu:637-717, 562-588, 444-454) of a bead
 // at (x,y,z) with deg bonded neighbours q[0..deg) in ascending bead order.
@@ -101,7 +110,7 @@ __device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
 // Same FP32 expression (explicit fma) as the oracle's move_bead().  Returns
 // whether the move is accepted; (px,py,pz) is the final position and cell the
 // final cell index.
-template <int MAXDEG>
+template <int MAXDEG, int FOLD = -1>
 __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, float z, const float* qx,
                                       const float* qy, const float* qz, int deg, float cc, float ac4, float n0,
                                       float n1, float n2, uint32_t aw, const float* __restrict__ w_t, float& px,
@@ -125,8 +134,8 @@ __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, flo
     const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
     const float fd = __fmaf_rn(fx, dx, __fmaf_rn(fy, dy, __fmul_rn(fz, dz)));
     const float deb = __fmul_rn(ac4, __fmaf_rn(cc, d2, __fmul_rn(-2.0f, fd)));
-    const int c_old = cell_of(c, x, y, z);
-    const int c_new = cell_of(c, px, py, pz);
+    const int c_old = cell_of<FOLD>(c, x, y, z);
+    const int c_new = cell_of<FOLD>(c, px, py, pz);
     const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + c_new), __ldg(w_t + c_old)), deb);
     // log(u) >= -23 ln2 > -17 for every u the generator yields: dE >= 17 rejects
     bool acc;
@@ -202,8 +211,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
         MoveConsts c;
         c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
         c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
-        c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
-        c.pow2 = is_pow2(c.nx) && is_pow2(c.ny) && is_pow2(c.nz);
+        load_fold(c, S);
         const uint32_t len_magic = Ap->len_magic;
         for (int i = tid; i < L; i += T) {
             if (LINEAR) {
@@ -397,8 +405,7 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
         MoveConsts c;
         c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
         c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
-        c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
-        c.pow2 = is_pow2(c.nx) && is_pow2(c.ny) && is_pow2(c.nz);
+        load_fold(c, S);
         const uint32_t len_magic = Ap->len_magic;
         const int64_t g0 = t.bead0 + (int64_t)c_begin * L;
         float* gx = S->x + g0;
@@ -535,7 +542,7 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
 #ifndef SCMF_REG_MIN_BLOCKS
 #define SCMF_REG_MIN_BLOCKS 3
 #endif
-template <int MODE, bool ANY_FLAT>
+template <int MODE, bool ANY_FLAT, int FOLD>
 __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const MoveTile* __restrict__ tiles,
                                                                         const int32_t* __restrict__ list, int n_list,
                                                                         unsigned* __restrict__ acc_part) {
@@ -562,8 +569,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
         MoveConsts c;
         c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
         c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
-        c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
-        c.pow2 = is_pow2(c.nx) && is_pow2(c.ny) && is_pow2(c.nz);
+        load_fold(c, S);
         const int64_t NC = S->n_cells;
         uint32_t* cnt = S->counts[MODE == kMoveGrid ? (S->cur ^ 1u) : S->cur];
         const bool c16 = S->count16 != 0;
@@ -604,11 +610,11 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
             }
             if (MODE == kGridOnly) {
                 if (live) {
-                    const int64_t ie = (int64_t)type_e * NC + cell_of(c, xe, ye, ze);
+                    const int64_t ie = (int64_t)type_e * NC + cell_of<FOLD>(c, xe, ye, ze);
                     if (c16) atomicAdd(cnt + (ie >> 1), 1u << ((ie & 1) * 16)); else atomicAdd(cnt + ie, 1u);
                 }
                 if (has_o) {
-                    const int64_t io = (int64_t)type_o * NC + cell_of(c, xo, yo, zo);
+                    const int64_t io = (int64_t)type_o * NC + cell_of<FOLD>(c, xo, yo, zo);
                     if (c16) atomicAdd(cnt + (io >> 1), 1u << ((io & 1) * 16)); else atomicAdd(cnt + io, 1u);
                 }
                 continue;
@@ -637,7 +643,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     normals3_spare(w, n0, n1, n2, spare);
                     float px, py, pz;
                     int cell;
-                    const bool acc = trial<2>(c, xe, ye, ze, qx, qy, qz, deg, deg == 2 ? cc2 : (deg == 1 ? cc1 : 0.0f),
+                    const bool acc = trial<2, FOLD>(c, xe, ye, ze, qx, qy, qz, deg, deg == 2 ? cc2 : (deg == 1 ? cc1 : 0.0f),
                                               deg == 2 ? ac42 : (deg == 1 ? ac41 : 0.0f), n0, n1, n2, accept_word(w),
                                               omega + (int64_t)type_e * NC, px, py, pz, cell);
                     if (acc) { xe = px; ye = py; ze = pz; }
@@ -677,7 +683,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     normals3_odd(spare, w, n0, n1, n2);
                     float px, py, pz;
                     int cell;
-                    const bool acc = trial<2>(c, xo, yo, zo, qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
+                    const bool acc = trial<2, FOLD>(c, xo, yo, zo, qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
                                               deg == 2 ? ac42 : ac41, n0, n1, n2, accept_word(w),
                                               omega + (int64_t)type_o * NC, px, py, pz, cell);
                     if (acc) { xo = px; yo = py; zo = pz; }
@@ -1251,6 +1257,15 @@ int configure_kernels() {
     return (int)e;
 }
 
+template <int MODE, bool FLAT>
+static void launch_reg(int fold, int blocks, int threads, cudaStream_t st, const MoveTile* tiles, const int32_t* list,
+                       int n, unsigned* acc) {
+    if (fold == 0)
+        k_sweep_reg<MODE, FLAT, 0><<<blocks, threads, 0, st>>>(tiles, list, n, acc);
+    else
+        k_sweep_reg<MODE, FLAT, -1><<<blocks, threads, 0, st>>>(tiles, list, n, acc);
+}
+
 template <int MODE>
 static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, LaunchShape sh, unsigned* acc,
                           cudaStream_t st) {
@@ -1262,11 +1277,11 @@ static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, L
         const int n_warp = sh.n_flat > 0 ? sh.n_warp : n_tiles;
         const int32_t* warp_list = sh.n_flat > 0 ? sh.warp_list : nullptr;
         if (n_warp > 0 && sh.part != 2)
-            k_sweep_reg<MODE, false><<<sh.blocks > 0 ? min(sh.blocks, n_warp) : n_warp, sh.threads, 0, st>>>(
-                tiles, warp_list, n_warp, acc);
+            launch_reg<MODE, false>(sh.fold, sh.blocks > 0 ? min(sh.blocks, n_warp) : n_warp, sh.threads, st, tiles,
+                                    warp_list, n_warp, acc);
         if (sh.n_flat > 0 && sh.part != 1)
-            k_sweep_reg<MODE, true><<<sh.blocks > 0 ? min(sh.blocks, sh.n_flat) : sh.n_flat, sh.threads, 0, st>>>(
-                tiles, sh.flat_list, sh.n_flat, acc);
+            launch_reg<MODE, true>(sh.fold, sh.blocks > 0 ? min(sh.blocks, sh.n_flat) : sh.n_flat, sh.threads, st,
+                                   tiles, sh.flat_list, sh.n_flat, acc);
     } else if (sh.linear) {
         // per-warp slice: ceil(chains per tile / warps) chains of the longest length
         const int nw = sh.threads / 32;
