@@ -135,6 +135,8 @@ typedef struct scmf_stats {
 /* Allocates and owns all device memory of the system (initialize_structure_GPU,
  * init_config.cu:737-854).  cuda_stream may be NULL for a private stream. */
 scmf_status scmf_system_create(const scmf_spec* spec, void* cuda_stream, scmf_system** out);
+/* A system that still belongs to a batch is freed when the last such batch is
+ * destroyed; its handle must not be used after this call either way. */
 void scmf_system_destroy(scmf_system* sys);
 scmf_status scmf_system_get_info(const scmf_system* sys, scmf_spec_info* out);
 scmf_status scmf_system_stream(const scmf_system* sys, void** cuda_stream);

@@ -360,6 +360,10 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
 
 void scmf_system_destroy(scmf_system* s) {
     if (!s) return;
+    if (s->batch_refs > 0) {  // a batch's plan still points at it: free with the last batch
+        s->destroy_pending = true;
+        return;
+    }
     cudaStreamSynchronize(s->stream);
     free_system(s);
 }
@@ -586,13 +590,19 @@ scmf_status scmf_batch_create(scmf_system* const* systems, int32_t n, const scmf
                 delete b;
                 return fail(SCMF_E_INVALID, "system %d appears twice", i);
             }
+        if (systems[i]->destroy_pending) {
+            delete b;
+            return fail(SCMF_E_INVALID, "system %d has been destroyed", i);
+        }
         b->systems.push_back(systems[i]);
     }
+    for (auto* s : b->systems) ++s->batch_refs;  // released by scmf_batch_destroy
     if (stream) {
         b->stream = (cudaStream_t)stream;
     } else {
         if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
-            delete b;
+            b->stream = nullptr;
+            scmf_batch_destroy(b);
             return fail(SCMF_E_CUDA, "cudaStreamCreate failed");
         }
         b->own_stream = true;
@@ -635,9 +645,15 @@ scmf_status scmf_batch_get_tune(const scmf_batch* b, scmf_tune* out) {
 
 void scmf_batch_destroy(scmf_batch* b) {
     if (!b) return;
-    cudaStreamSynchronize(b->stream);
+    if (b->stream) cudaStreamSynchronize(b->stream);
     b->plan.release();
+    if (b->stream) cudaStreamSynchronize(b->stream);  // the plan's stream-ordered frees
     if (b->own_stream) cudaStreamDestroy(b->stream);
+    for (auto* s : b->systems)
+        if (--s->batch_refs == 0 && s->destroy_pending) {
+            s->destroy_pending = false;
+            scmf_system_destroy(s);
+        }
     delete b;
 }
 

@@ -133,6 +133,8 @@ struct scmf_system {
     float* d_ref = nullptr;      // reference snapshot for displacements, SoA (lazy)
     double* d_obs = nullptr;     // per-tile observable partials (lazy)
     unsigned long long* d_check = nullptr;  // validation counters (lazy)
+    int batch_refs = 0;           // batches whose plans point at this system
+    bool destroy_pending = false; // destroyed by the caller while still in a batch
     std::vector<scmf::ArchHost> archs;
     std::vector<scmf::ArchDev> h_arch;  // host image of d_arch
     scmf::DevPlan plan;                  // default work plan of this system alone

@@ -226,3 +226,27 @@ def test_autotune_keeps_state(nb):
     b.close()
     for s in systems:
         s.close()
+
+
+def test_destroying_a_batched_system_is_deferred(nb):
+    """A system destroyed while a batch still holds it stays alive until the
+    batch is destroyed, so the batch keeps stepping correctly; it cannot join
+    a new batch."""
+    specs = nb.spec.batched_mix(3, mix_seed=13, edge_scale=0.25)
+    systems = [nb.System(sp) for sp in specs]
+    for s in systems:
+        s.init_coords()
+    b = nb.Batch(systems)
+    held = systems[0].handle.value
+    systems[0].close()                       # deferred: the batch still points at it
+    b.step(3)
+    orc = oracle_for(specs[1])
+    orc.step(3)
+    compare_state(systems[1], orc, "batch member after another member was destroyed")
+    with pytest.raises(nb.ScmfError):
+        import ctypes as C
+        arr = (C.c_void_p * 1)(held)
+        nb._lib.check(nb.lib().scmf_batch_create(arr, 1, None, None, C.byref(C.c_void_p())))
+    b.close()                                # frees systems[0] now
+    for s in systems[1:]:
+        s.close()
