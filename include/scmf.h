@@ -391,6 +391,9 @@ scmf_status scmf_server_cancel(scmf_server* s, uint64_t id);
  * after timeout_ms (the requests keep running). */
 scmf_status scmf_server_drain(scmf_server* s, int32_t timeout_ms);
 double scmf_server_now(const scmf_server* s);
+/* Stops the server: queued requests are dropped, running ones stop at their
+ * round boundary, their device memory is freed, and results not yet polled
+ * are discarded.  Drain first (scmf_server_drain) to finish outstanding work. */
 void scmf_server_destroy(scmf_server* s);
 
 #ifdef __cplusplus

@@ -127,7 +127,8 @@ void scmf_server::admit_loop() {
         {
             std::unique_lock<std::mutex> lk(mu);
             for (;;) {
-                if (stop && queue.empty()) {
+                if (stop) {  // shutting down: queued requests are dropped
+                    queue.clear();
                     admission_done = true;
                     cv_ready.notify_all();
                     return;
@@ -193,7 +194,7 @@ void scmf_server::round_loop() {
                 plan_valid = false;
             }
             for (auto& a : active)
-                if (cancelled.count(a.req.id)) drop.push_back(a.req.id);
+                if (stop || cancelled.count(a.req.id)) drop.push_back(a.req.id);
         }
         if (!drop.empty()) {
             std::vector<Active> keep;

@@ -247,3 +247,20 @@ def test_server_cancel_and_drain(nb):
         assert r["status"] == 0 and r["sweeps_done"] == K
         assert_counts_equal(r["counts"], cnt, "served counts after cancellations")
         assert r["accepts"] == st["total_accepts"]
+
+
+def test_server_destroy_cancels_outstanding_work(nb):
+    """Closing a server with requests queued and running returns at the next
+    round boundary instead of finishing them all."""
+    from new_arch_b200.server import Server
+    from new_arch_b200.spec import diblock_melt
+    sp = diblock_melt(3000, 16, 0.5, (16, 16, 16), 20.0, 50.0, seed=9)
+    srv = Server(int(sp.device_bytes() * 2.5), sweeps_per_round=2)
+    for _ in range(20):
+        srv.submit(sp, 200_000)                      # hours of work if it all ran
+    t0 = time.time()
+    while srv.pending()[1] < 1 and time.time() - t0 < 30:
+        time.sleep(0.001)
+    t0 = time.time()
+    srv.close()
+    assert time.time() - t0 < 10
