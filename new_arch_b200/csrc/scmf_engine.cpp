@@ -84,6 +84,9 @@ scmf_status validate_spec(const scmf_spec& s) {
     if (s.n_types < 1 || s.n_types > kMaxTypes) return fail(SCMF_E_INVALID, "n_mono_types %d not in [1,%d]", s.n_types, kMaxTypes);
     if (s.nx < 1 || s.ny < 1 || s.nz < 1) return fail(SCMF_E_INVALID, "grid %d x %d x %d invalid", s.nx, s.ny, s.nz);
     if ((int64_t)s.nx * s.ny * s.nz > ((int64_t)1 << 30)) return fail(SCMF_E_INVALID, "grid too large");
+    // the FP32 cell fold is exact while |x / dx| < 2^22: keep whole boxes well inside that
+    if (s.nx > (1 << 20) || s.ny > (1 << 20) || s.nz > (1 << 20))
+        return fail(SCMF_E_INVALID, "grid axis longer than %d cells", 1 << 20);
     if (!(s.lx > 0 && s.ly > 0 && s.lz > 0)) return fail(SCMF_E_INVALID, "box lengths must be positive");
     if ((int)s.xn.size() != s.n_types * s.n_types) return fail(SCMF_E_INVALID, "xn matrix not set");
     if (s.p.reference_nbeads < 1) return fail(SCMF_E_INVALID, "reference_nbeads must be >= 1");
@@ -95,6 +98,7 @@ scmf_status validate_spec(const scmf_spec& s) {
     int64_t beads = 0, chains = 0;
     for (const auto& a : s.archs) {
         if (a.length < 1 || a.length > kMaxLength) return fail(SCMF_E_INVALID, "chain length %d not in [1,%d]", a.length, kMaxLength);
+        if (a.n_chains < 0) return fail(SCMF_E_INVALID, "negative chain count %d", a.n_chains);
         beads += (int64_t)a.length * a.n_chains;
         chains += a.n_chains;
     }

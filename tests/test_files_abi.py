@@ -106,6 +106,22 @@ def test_spec_validation_errors():
     rc = _lib.lib().scmf_system_create(h, None, C.byref(out))
     _lib.lib().scmf_spec_destroy(h)
     assert rc == -1 and b"16-bit" in _lib.lib().scmf_last_error()
+    # an axis longer than the exact range of the FP32 fold allows
+    long_axis = diblock_melt(10, 8, 0.5, ((1 << 20) + 1, 2, 1), 10.0, 50.0)
+    h = long_axis.to_c()
+    rc = _lib.lib().scmf_system_create(h, None, C.byref(out))
+    _lib.lib().scmf_spec_destroy(h)
+    assert rc == -1 and b"grid axis" in _lib.lib().scmf_last_error()
+    # a negative chain count is refused where it is given
+    neg = diblock_melt(10, 8, 0.5, (4, 4, 4), 10.0, 50.0)
+    neg.archs[0].n_chains = -3
+    with pytest.raises(nb.ScmfError) as e:
+        h = neg.to_c()
+        try:
+            _lib.check(_lib.lib().scmf_system_create(h, None, C.byref(out)))
+        finally:
+            _lib.lib().scmf_spec_destroy(h)
+    assert e.value.code == -1
 
 
 @pytest.mark.skipif(HAS_GPU, reason="checks the no-device error path")
