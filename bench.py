@@ -247,14 +247,13 @@ def run_ours(args):
     t0 = time.perf_counter()
     s.set_coords(host_in)
     for _ in range(args.steps):
-        s.step(1)
-        s.sweep_stats()
+        s.step_stats(1)
     cnt = s.counts()
     e2e_s = allmax(time.perf_counter() - t0)
     e2e = {"value": whole_job_rate(beads_all, args.steps, e2e_s), "unit": UNIT,
            "h2d_bytes_per_step": xyz.nbytes / args.steps,
            "d2h_bytes_per_step": (64 * args.steps + cnt.nbytes) / args.steps,
-           "how": "wall clock around scmf_set_coords(pinned host xyz) + K x (scmf_step(1) + scmf_get_sweep_stats) + scmf_get_counts"}
+           "how": "wall clock around scmf_set_coords(pinned host xyz) + K x scmf_step_stats(1) + scmf_get_counts"}
     s.close()
     del pinned
 

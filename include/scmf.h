@@ -173,6 +173,10 @@ scmf_status scmf_get_stats(const scmf_system* sys, scmf_stats* out);
  * one small device-to-host read; e_bond is NaN unless it is current (it is
  * computed on demand by scmf_get_stats). */
 scmf_status scmf_get_sweep_stats(const scmf_system* sys, scmf_stats* out);
+/* scmf_step followed by scmf_get_sweep_stats with one device read and one
+ * wait: the loop of a driver that reports every sweep (test.cpp:45-68 prints
+ * per check step) costs one host round trip per call instead of three. */
+scmf_status scmf_step_stats(scmf_system* sys, int32_t n_sweeps, scmf_stats* out);
 
 /* Diagnostics: evaluates the device arithmetic (Philox4x32-10 with counter
  * (c0,c1,c2,c3) = (i, 0, 0, 0) and the given key, then log(u01(w.x)),

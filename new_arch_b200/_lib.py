@@ -126,6 +126,7 @@ SIGNATURES = {
     "scmf_set_omega": (_i32, [_vp, _pf32, _sz]),
     "scmf_get_stats": (_i32, [_vp, C.POINTER(Stats)]),
     "scmf_get_sweep_stats": (_i32, [_vp, C.POINTER(Stats)]),
+    "scmf_step_stats": (_i32, [_vp, _i32, C.POINTER(Stats)]),
     "scmf_debug_math": (_i32, [_u32, _u32, _i32, _pu32, _pf32, _pf32, _pf32, _pf32]),
     "scmf_update_omega_noalloc": (_i32, [_vp, _vp, _i32, _i64, _f64, _pf64, _i32, _i32, _vp, _vp]),
     "scmf_write_density": (_i32, [_vp, C.c_char_p, _i64]),

@@ -553,6 +553,23 @@ scmf_status scmf_get_sweep_stats(const scmf_system* s, scmf_stats* o) {
     return SCMF_OK;
 }
 
+scmf_status scmf_step_stats(scmf_system* s, int32_t n, scmf_stats* o) {
+    if (!s || !o || n < 0) return fail(SCMF_E_INVALID, "bad argument");
+    RET(s->plan.run_sweeps(s->stream, n));
+    SysDev d;
+    RET(fetch_sysdev(s, &d));  // queued behind the sweeps: one wait for both
+    if (d.error_word) return fail(SCMF_E_DEVICE, "kernel error word 0x%x", d.error_word);
+    std::memset(o, 0, sizeof *o);
+    o->step = d.step;
+    o->last_accepts = d.last_accepts;
+    o->total_accepts = d.total_accepts;
+    o->total_moves = d.total_moves;
+    o->e_bond = d.e_bond_step == d.step + 1u ? d.e_bond : std::nan("");
+    o->e_field = d.e_field;
+    o->error_word = d.error_word;
+    return SCMF_OK;
+}
+
 scmf_status scmf_get_stats(const scmf_system* cs, scmf_stats* o) {
     scmf_system* s = const_cast<scmf_system*>(cs);
     if (!s || !o) return fail(SCMF_E_INVALID, "NULL argument");

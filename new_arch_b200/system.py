@@ -117,6 +117,12 @@ class System:
     def step(self, n_sweeps: int = 1) -> None:
         check(lib().scmf_step(self._h, int(n_sweeps)))
 
+    def step_stats(self, n_sweeps: int = 1) -> dict:
+        """n sweeps, then the statistics of the last one, in one round trip."""
+        st = _lib.Stats()
+        check(lib().scmf_step_stats(self._h, int(n_sweeps), C.byref(st)))
+        return {k: getattr(st, k) for k, _ in _lib.Stats._fields_ if k != "reserved"}
+
     def step_async(self, n_sweeps: int = 1) -> None:
         check(lib().scmf_step_async(self._h, int(n_sweeps)))
 

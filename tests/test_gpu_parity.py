@@ -250,3 +250,17 @@ def test_destroying_a_batched_system_is_deferred(nb):
     b.close()                                # frees systems[0] now
     for s in systems[1:]:
         s.close()
+
+
+def test_step_stats_equals_step_then_sweep_stats(nb):
+    spec = nb.spec.diblock_melt(500, 16, 0.4, (8, 8, 8), 20.0, 50.0, seed=21)
+    with nb.System(spec) as a, nb.System(spec) as b:
+        a.init_coords()
+        b.init_coords()
+        for n in (1, 3):
+            sa = a.step_stats(n)
+            b.step(n)
+            sb = b.sweep_stats()
+            for k in ("step", "last_accepts", "total_accepts", "total_moves", "e_field", "error_word"):
+                assert sa[k] == sb[k], k
+        assert_counts_equal(a.counts(), b.counts(), "step_stats counts")
