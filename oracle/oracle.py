@@ -71,6 +71,7 @@ def lib():
     L.orc_average_get.restype = C.c_uint64
     L.orc_average_get.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.orc_analysis_reference.argtypes = [vp]
+    L.orc_set_fault.argtypes = [vp, i32]
     L.orc_analyze.restype = i32
     L.orc_analyze.argtypes = [vp, i32, C.POINTER(C.c_double)]
     L.orc_philox4x32_10.argtypes = [u32p, u32p, u32p]
@@ -214,6 +215,10 @@ class OracleSystem:
         out = np.zeros(self.n_types * self.n_cells, dtype=np.uint64)
         n = lib().orc_average_get(self._h, _p(out, C.c_uint64))
         return out, int(n)
+
+    def set_fault(self, no_smc: bool):
+        """Plant a known mistake (drop the smart-MC correction) to test the tests."""
+        lib().orc_set_fault(self._h, int(bool(no_smc)))
 
     def analysis_reference(self):
         lib().orc_analysis_reference(self._h)

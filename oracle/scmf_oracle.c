@@ -208,6 +208,7 @@ struct orc_system {
     uint32_t avg_every;
     uint64_t avg_samples;
     float *rx, *ry, *rz;
+    int fault_no_smc;  /* planted mistake for tests: plain Metropolis on the bond energy */
 };
 
 static int g_threads = 1;
@@ -470,7 +471,15 @@ static inline int move_bead(const orc_system* s, const orc_arch* a, int b, float
     const float* W = s->omega + (int64_t)t * s->n_cells;
     const float w_old = W[cell_of(s, x, y, z)];
     const float w_new = W[cell_of(s, px, py, pz)];
-    const float dE = (w_new - w_old) + dE_closed(c, ac4, fx, fy, fz, dx, dy, dz);
+    float eb;
+    if (s->fault_no_smc) {  /* the bond energy change alone, (c/2)|d|^2 - f.d, without the smart-MC correction */
+        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float fd = fmaf(fx, dx, fmaf(fy, dy, fz * dz));
+        eb = fmaf(0.5f * c, d2, -fd);
+    } else {
+        eb = dE_closed(c, ac4, fx, fy, fz, dx, dy, dz);
+    }
+    const float dE = (w_new - w_old) + eb;
     /* Metropolis: accept if dE < 0, else if log(u) < -dE.  log(u) >= -23 ln2
      * > -17 for every u the generator yields, so dE >= 17 always rejects. */
     int acc;
@@ -609,6 +618,8 @@ void orc_step(orc_system* s, int n) {
 
 /* Time-averaged density: the counts of the final positions of every sweep s
  * with s % every == 0 are summed (average_field_unified, struct.h:234). */
+void orc_set_fault(orc_system* s, int no_smc) { s->fault_no_smc = no_smc; }
+
 void orc_average_start(orc_system* s, uint32_t every) {
     free(s->avg);
     s->avg = NULL;

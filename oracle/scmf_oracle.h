@@ -81,6 +81,10 @@ uint64_t orc_average_get(const orc_system* s, uint64_t* sums);
 
 /* chain observables (means in double): out[15] = re2 xyz, rg2 xyz, bond2 xyz,
  * msd xyz, msd_com xyz; displacements are NaN before orc_analysis_reference */
+/* Plants a known mistake (tests of the tests only): no_smc = 1 accepts moves
+ * by plain Metropolis on the bond energy, dropping the smart-MC correction. */
+void orc_set_fault(orc_system* s, int no_smc);
+
 void orc_analysis_reference(orc_system* s);
 int  orc_analyze(const orc_system* s, int arch, double* out);
 

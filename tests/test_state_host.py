@@ -165,3 +165,34 @@ def test_spec_hash_tracks_trajectory_parameters():
     assert hash_of(a) != hash_of(diblock_melt(30, 8, 0.5, (4, 4, 4), 11.0, 50.0, seed=1))
     assert hash_of(a) != hash_of(diblock_melt(31, 8, 0.5, (4, 4, 4), 10.0, 50.0, seed=1))
     assert hash_of(a) != hash_of(diblock_melt(30, 8, 0.5, (4, 4, 5), 10.0, 50.0, seed=1))
+
+
+# ------------------------------------------------ physics of the algorithm
+def _ideal_chain_bond2(fault: bool) -> float:
+    """<|b|^2> of field-free chains relaxed by the oracle from a third of the
+    equilibrium bond length; the exact value is 3 / (2k)."""
+    from oracle.oracle import set_threads
+    import os
+    spec = diblock_melt(1500, 8, 0.5, (8, 8, 8), 0.0, 0.0, seed=77, smc_a=0.1)
+    spec.archs[0].init_sigma = 0.7 / np.sqrt(3.0) / 3.0
+    set_threads(os.cpu_count() or 1)
+    try:
+        o = _oracle(spec)
+        o.set_fault(fault)
+        o.step(600)
+        vals = []
+        for _ in range(20):
+            o.step(20)
+            vals.append(o.analyze(0)["bond2"].sum())
+    finally:
+        set_threads(1)
+    return float(np.mean(vals)) / (3.0 / (2.0 * spec.harmonic_normb))
+
+
+def test_ideal_chain_statistics_detect_a_wrong_acceptance():
+    """The statistics that the GPU physics test checks (tests/test_gpu_physics.py)
+    hold for the oracle's algorithm and fail for a planted mistake: plain
+    Metropolis on the bond energy with the drifted proposal, i.e. without the
+    smart-MC correction."""
+    assert abs(_ideal_chain_bond2(False) - 1.0) < 0.02
+    assert abs(_ideal_chain_bond2(True) - 1.0) > 0.05
