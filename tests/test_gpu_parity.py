@@ -264,3 +264,27 @@ def test_step_stats_equals_step_then_sweep_stats(nb):
             for k in ("step", "last_accepts", "total_accepts", "total_moves", "e_field", "error_word"):
                 assert sa[k] == sb[k], k
         assert_counts_equal(a.counts(), b.counts(), "step_stats counts")
+
+
+def test_edge_shapes(nb):
+    """Single beads (no bonds), dimers, trimers, an architecture with no chains,
+    and a system of a single chain: bit-exact against the oracle."""
+    from new_arch_b200.spec import SystemSpec, cell_units, diblock_arch, homopolymer_arch, interaction_matrix
+    k, sig = cell_units()
+    cases = {
+        "mixed short": [homopolymer_arch(1, 0, 300, sig), diblock_arch(2, 0.5, 200, sig),
+                        diblock_arch(3, 0.34, 150, sig), homopolymer_arch(5, 1, 0, sig)],
+        "one chain": [diblock_arch(32, 0.5, 1, sig)],
+        "one bead": [homopolymer_arch(1, 1, 1, sig)],
+    }
+    for name, archs in cases.items():
+        spec = SystemSpec(2, 5, 4, 3, 5.0, 4.0, 3.0, interaction_matrix(2, 20.0, 50.0), 8, k, 0.5, 404,
+                          nb.HAM_SCMF0, nb.FIELD_EVERY, 32, archs)
+        with nb.System(spec) as s:
+            s.init_coords()
+            orc = oracle_for(spec)
+            compare_state(s, orc, name + " init")
+            s.step(6)
+            orc.step(6)
+            compare_state(s, orc, name)
+            assert int(s.counts().sum()) == spec.n_beads
