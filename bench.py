@@ -232,10 +232,12 @@ def run_ours(args):
     beads_all = gather_ints(spec.n_beads, dist, "cuda")
     value = whole_job_rate(beads_all, args.steps, ms_total / 1e3)
     peak, peak_kind = measured_peaks()
-    alg_bytes = 24 * spec.n_beads + 4 * spec.n_types * spec.n_cells          # move+grid kernel per launch
+    # move+grid kernel per launch: read and write x, y, z (counts change only for
+    # accepted moves that leave their cell, ~1 % of beads here: not counted)
+    alg_bytes = 24 * spec.n_beads
     achieved = alg_bytes / (ms_move / args.steps / 1e3) / 1e9
     traffic = profiled_traffic("sweep_large_system")
-    field_bytes = 12 * spec.n_types * spec.n_cells                          # read new counts, write omega, clear old counts
+    field_bytes = 8 * spec.n_types * spec.n_cells                           # read counts, write omega
     field_gbs = field_bytes / (ms_field / args.steps / 1e3) / 1e9
 
     # ---- end to end through the C ABI with host buffers

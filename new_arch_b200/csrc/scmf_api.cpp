@@ -77,8 +77,13 @@ scmf_status regrid(scmf_system* s) {
     sh.blocks = 0;
     CKL(launch_sweep(kGridOnly, s->plan.d_move, s->plan.n_move, s->plan.max_tile_beads, s->plan.max_length, sh,
                      s->plan.d_acc, s->stream));
+    s->counts_stale = false;
     return SCMF_OK;
 }
+
+// Fused sweeps move counts cell to cell and so need counts that are the grid
+// of the positions; only a move-only call (scmf_smc_move) leaves them behind.
+scmf_status fresh_counts(scmf_system* s) { return s->counts_stale ? regrid(s) : SCMF_OK; }
 
 scmf_status field_now(scmf_system* s) {
     LaunchShape sh = s->plan.field_shape();
@@ -422,6 +427,7 @@ scmf_status scmf_set_step(scmf_system* s, uint64_t step) {
 
 scmf_status scmf_step_async(scmf_system* s, int32_t n) {
     if (!s || n < 0) return fail(SCMF_E_INVALID, "bad argument");
+    RET(fresh_counts(s));
     return s->plan.run_sweeps(s->stream, n);
 }
 
@@ -433,6 +439,7 @@ scmf_status scmf_step(scmf_system* s, int32_t n) {
 
 scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float* ms_field, float* ms_total) {
     if (!s || n < 0 || !ms_move || !ms_field || !ms_total) return fail(SCMF_E_INVALID, "bad argument");
+    RET(fresh_counts(s));
     *ms_move = 0.0f;
     *ms_field = 0.0f;
     *ms_total = 0.0f;
@@ -475,6 +482,7 @@ scmf_status scmf_smc_move(scmf_system* s, int32_t n) {
                          s->plan.d_acc, s->stream));
         RET(s->plan.enqueue_close(kCloseMove | kCloseAdvance, s->stream));
     }
+    if (n > 0) s->counts_stale = true;  // like the reference, counts wait for reset_density_fields
     CK(cudaStreamSynchronize(s->stream));
     return check_error_word(s);
 }
@@ -555,6 +563,7 @@ scmf_status scmf_get_sweep_stats(const scmf_system* s, scmf_stats* o) {
 
 scmf_status scmf_step_stats(scmf_system* s, int32_t n, scmf_stats* o) {
     if (!s || !o || n < 0) return fail(SCMF_E_INVALID, "bad argument");
+    RET(fresh_counts(s));
     RET(s->plan.run_sweeps(s->stream, n));
     SysDev d;
     RET(fetch_sysdev(s, &d));  // queued behind the sweeps: one wait for both
@@ -643,8 +652,10 @@ static scmf_status batch_sync_members(scmf_batch* b) {
 
 scmf_status scmf_batch_step_async(scmf_batch* b, int32_t n) {
     if (!b || n < 0) return fail(SCMF_E_INVALID, "bad argument");
-    for (auto* s : b->systems)
+    for (auto* s : b->systems) {
+        RET(fresh_counts(s));
         if (s->stream != b->stream) CK(cudaStreamSynchronize(s->stream));
+    }
     return b->plan.run_sweeps(b->stream, n);
 }
 

@@ -133,6 +133,7 @@ struct scmf_system {
     float* d_ref = nullptr;      // reference snapshot for displacements, SoA (lazy)
     double* d_obs = nullptr;     // per-tile observable partials (lazy)
     unsigned long long* d_check = nullptr;  // validation counters (lazy)
+    bool counts_stale = false;    // moved without counts (scmf_smc_move): regrid before a fused sweep
     int batch_refs = 0;           // batches whose plans point at this system
     bool destroy_pending = false; // destroyed by the caller while still in a batch
     std::vector<scmf::ArchHost> archs;
@@ -157,6 +158,7 @@ scmf_status write_density_file(const scmf_system* s, const char* path, int64_t s
 scmf_status alloc_scratch(void** p, size_t bytes, cudaStream_t st);  // device buffer, 256-byte rounded
 size_t counts_bytes(const scmf_system* s);
 scmf_status regrid(scmf_system* s);         // counts of the current positions into counts[0], cur = 0
+scmf_status fresh_counts(scmf_system* s);   // regrid if a move-only call left the counts stale
 scmf_status field_now(scmf_system* s);      // omega of the current counts (always updated)
 scmf_status ensure_aos(scmf_system* s);     // AoS staging buffer
 scmf_status check_error_word(const scmf_system* s);

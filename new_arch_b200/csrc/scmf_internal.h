@@ -10,9 +10,11 @@
 //                                      key), so chains can be reordered in space
 //                                      without changing any result.
 //   counts[2]    uint32[n_types*n_cells] (or uint16 pairs)  per-type cell counts,
-//                                      [type][z][y][x]; double-buffered so the
-//                                      fused sweep accumulates into one buffer
-//                                      while the field step clears the other.
+//                                      [type][z][y][x].  counts[cur] is kept the
+//                                      grid of the positions: a fused sweep
+//                                      moves a count for each accepted move that
+//                                      leaves its cell.  The other buffer is
+//                                      zero between calls (validation scratch).
 //   omega        float[n_types*n_cells]  quasi-instantaneous field.
 // plus a SysDev descriptor in device memory holding constants, the sweep
 // counter and the statistics accumulators.
@@ -123,7 +125,7 @@ enum SweepMode : int { kMoveOnly = 0, kMoveGrid = 1, kGridOnly = 2 };
 enum CloseMode : int {
     kCloseMove = 1, kCloseField = 2, kCloseBond = 4, kCloseFlip = 8, kCloseAdvance = 16,
     kCloseAverage = 32,  // count a time-averaged density sample when the sweep took one
-    kSweepClose = kCloseMove | kCloseField | kCloseFlip | kCloseAdvance | kCloseAverage
+    kSweepClose = kCloseMove | kCloseField | kCloseAdvance | kCloseAverage
 };
 
 // Per-tile partial sums of the chain observables (k_observables), each over

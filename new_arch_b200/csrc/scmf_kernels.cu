@@ -114,7 +114,7 @@ template <int MAXDEG, int FOLD = -1>
 __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, float z, const float* qx,
                                       const float* qy, const float* qz, int deg, float cc, float ac4, float n0,
                                       float n1, float n2, uint32_t aw, const float* __restrict__ w_t, float& px,
-                                      float& py, float& pz, int& cell) {
+                                      float& py, float& pz, int& cell_old, int& cell_new) {
     const float k2 = c.k2, A = c.A, R = c.R;
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
 #pragma unroll
@@ -145,8 +145,23 @@ __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, flo
         acc = log_f(u01(aw)) < -dE;
     else
         acc = false;
-    cell = acc ? c_new : c_old;
+    cell_old = c_old;
+    cell_new = c_new;
     return acc;
+}
+
+// Counts are kept as the grid of the current positions: a fused sweep moves
+// one count from the old to the new cell of every accepted move that leaves
+// its cell (typ = type * n_cells), instead of regridding every bead.
+__device__ __forceinline__ void count_move(uint32_t* cnt, bool c16, int64_t typ, int c_old, int c_new) {
+    const int64_t io = typ + c_old, in = typ + c_new;
+    if (c16) {
+        atomicSub(cnt + (io >> 1), 1u << ((io & 1) * 16));  // the cell holds this bead: no borrow
+        atomicAdd(cnt + (in >> 1), 1u << ((in & 1) * 16));
+    } else {
+        atomicSub(cnt + io, 1u);
+        atomicAdd(cnt + in, 1u);
+    }
 }
 
 // Philox block and normals of bead b of chain gc (odd beads also draw the
@@ -180,8 +195,9 @@ size_t sweep_smem_bytes(int max_tile_beads, int max_length) {
 }
 
 // One MC sweep over tiles of whole chains staged in shared memory.
-//   MODE kMoveOnly / kMoveGrid / kGridOnly: moves, moves + counts of the final
-//   positions into counts[cur^1], counts of the current positions into counts[cur].
+//   MODE kMoveOnly / kMoveGrid / kGridOnly: moves; moves keeping counts[cur]
+//   the grid of the positions (accepted moves that change cell move a count);
+//   counts of the current positions added into counts[cur] (a cleared buffer).
 //   LINEAR: every architecture of the launch is a linear chain (bonds i-i+1,
 //   even beads colour 0, odd beads colour 1); neighbours are computed, not looked up.
 template <int MODE, bool LINEAR>
@@ -251,7 +267,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
             const float* __restrict__ omega = S->omega;
             const int64_t NC = S->n_cells;
             const float cc2 = S->cdeg[2], ac42 = S->ac4deg[2];
-            uint32_t* cnt = S->counts[S->cur ^ 1u];
+            uint32_t* cnt = S->counts[S->cur];
             const bool c16 = S->count16 != 0;
             unsigned nacc = 0;
             for (int col = 0; col < Ap->n_colors; ++col) {
@@ -297,24 +313,18 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
                     float n0, n1, n2;
                     const uint32_t aw = bead_normals(__ldg(cid + cl), b, step, k0, k1, n0, n1, n2);
                     float px, py, pz;
-                    int cell;
+                    int c_old, c_new;
                     const bool acc = trial<LINEAR ? 2 : kMaxDeg>(c, sx[base + b], sy[base + b], sz[base + b], qx, qy,
                                                                  qz, deg, deg == 2 ? cc2 : S->cdeg[deg],
                                                                  deg == 2 ? ac42 : S->ac4deg[deg], n0, n1, n2, aw,
-                                                                 omega + (int64_t)type * NC, px, py, pz, cell);
+                                                                 omega + (int64_t)type * NC, px, py, pz, c_old, c_new);
                     if (acc) {
                         sx[base + b] = px;
                         sy[base + b] = py;
                         sz[base + b] = pz;
                     }
                     nacc += acc ? 1u : 0u;
-                    if (MODE == kMoveGrid) {
-                        const int64_t idx = (int64_t)type * NC + cell;
-                        if (c16)
-                            atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16));
-                        else
-                            atomicAdd(cnt + idx, 1u);
-                    }
+                    if (MODE == kMoveGrid && acc && c_new != c_old) count_move(cnt, c16, (int64_t)type * NC, c_old, c_new);
                 }
                 __syncthreads();
             }
@@ -323,8 +333,7 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
         }
 
         if (MODE == kGridOnly) {
-            const uint32_t buf = (MODE == kMoveGrid) ? (S->cur ^ 1u) : S->cur;
-            uint32_t* cnt = S->counts[buf];
+            uint32_t* cnt = S->counts[S->cur];
             const int64_t NC = S->n_cells;
             const bool c16 = S->count16 != 0;
             for (int i = tid; i < nb; i += T) {
@@ -421,7 +430,7 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
         }
         const uint8_t* __restrict__ types = Ap->types;
         const int64_t NC = S->n_cells;
-        uint32_t* cnt = S->counts[MODE == kMoveGrid ? (S->cur ^ 1u) : S->cur];
+        uint32_t* cnt = S->counts[S->cur];
         const bool c16 = S->count16 != 0;
         __syncwarp();
         if (MODE != kGridOnly) {
@@ -478,23 +487,17 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
                     }
                     const uint32_t aw = accept_word(w);
                     float px, py, pz;
-                    int cell;
+                    int c_old, c_new;
                     const bool acc = trial<2>(c, sx[me], sy[me], sz[me], qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
                                               deg == 2 ? ac42 : ac41, n0, n1, n2, aw, omega + (int64_t)type * NC, px,
-                                              py, pz, cell);
+                                              py, pz, c_old, c_new);
                     if (acc) {
                         sx[me] = px;
                         sy[me] = py;
                         sz[me] = pz;
                     }
                     nacc += acc ? 1u : 0u;
-                    if (MODE == kMoveGrid) {
-                        const int64_t idx = (int64_t)type * NC + cell;
-                        if (c16)
-                            atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16));
-                        else
-                            atomicAdd(cnt + idx, 1u);
-                    }
+                    if (MODE == kMoveGrid && acc && c_new != c_old) count_move(cnt, c16, (int64_t)type * NC, c_old, c_new);
                 }
                 __syncwarp();
             }
@@ -571,7 +574,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
         c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
         load_fold(c, S);
         const int64_t NC = S->n_cells;
-        uint32_t* cnt = S->counts[MODE == kMoveGrid ? (S->cur ^ 1u) : S->cur];
+        uint32_t* cnt = S->counts[S->cur];
         const bool c16 = S->count16 != 0;
         const float* __restrict__ omega = S->omega;
         const uint32_t step = S->step + 1u;
@@ -642,16 +645,14 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     float n0, n1, n2;
                     normals3_spare(w, n0, n1, n2, spare);
                     float px, py, pz;
-                    int cell;
+                    int c_old, c_new;
                     const bool acc = trial<2, FOLD>(c, xe, ye, ze, qx, qy, qz, deg, deg == 2 ? cc2 : (deg == 1 ? cc1 : 0.0f),
                                               deg == 2 ? ac42 : (deg == 1 ? ac41 : 0.0f), n0, n1, n2, accept_word(w),
-                                              omega + (int64_t)type_e * NC, px, py, pz, cell);
+                                              omega + (int64_t)type_e * NC, px, py, pz, c_old, c_new);
                     if (acc) { xe = px; ye = py; ze = pz; }
                     nacc += acc ? 1u : 0u;
-                    if (MODE == kMoveGrid) {
-                        const int64_t idx = (int64_t)type_e * NC + cell;
-                        if (c16) atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16)); else atomicAdd(cnt + idx, 1u);
-                    }
+                    if (MODE == kMoveGrid && acc && c_new != c_old)
+                        count_move(cnt, c16, (int64_t)type_e * NC, c_old, c_new);
                 }
             }
             // odd half-sweep
@@ -682,16 +683,14 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     float n0, n1, n2;
                     normals3_odd(spare, w, n0, n1, n2);
                     float px, py, pz;
-                    int cell;
+                    int c_old, c_new;
                     const bool acc = trial<2, FOLD>(c, xo, yo, zo, qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
                                               deg == 2 ? ac42 : ac41, n0, n1, n2, accept_word(w),
-                                              omega + (int64_t)type_o * NC, px, py, pz, cell);
+                                              omega + (int64_t)type_o * NC, px, py, pz, c_old, c_new);
                     if (acc) { xo = px; yo = py; zo = pz; }
                     nacc += acc ? 1u : 0u;
-                    if (MODE == kMoveGrid) {
-                        const int64_t idx = (int64_t)type_o * NC + cell;
-                        if (c16) atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16)); else atomicAdd(cnt + idx, 1u);
-                    }
+                    if (MODE == kMoveGrid && acc && c_new != c_old)
+                        count_move(cnt, c16, (int64_t)type_o * NC, c_old, c_new);
                 }
             }
             if (live) {
@@ -764,12 +763,11 @@ __device__ __forceinline__ double omega_of_cell(int nt, const uint32_t* cnt, flo
 // Scalar path: one cell (any count width, any alignment).
 template <int NT, bool FUSED>
 __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, float scale, bool lit, bool upd,
-                                             bool c16, const uint32_t* src32, uint32_t* clr32, float* W,
-                                             const float* cf, unsigned long long* avg) {
+                                             bool c16, const uint32_t* src32, float* W, const float* cf,
+                                             unsigned long long* avg) {
     constexpr int M = NT > 0 ? NT : kMaxTypes;
     const int nt = NT > 0 ? NT : n;
     const uint16_t* src16 = reinterpret_cast<const uint16_t*>(src32);
-    uint16_t* clr16 = reinterpret_cast<uint16_t*>(clr32);
     uint32_t cnt[M];
     float w[M];
 #pragma unroll
@@ -783,15 +781,7 @@ __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, fl
     const double ef = omega_of_cell<NT>(nt, cnt, scale, lit, upd, w, cf);
 #pragma unroll
     for (int t = 0; t < M; ++t) {
-        if (t < nt) {
-            if (upd) W[t * NC + cell] = w[t];
-            if (FUSED) {
-                if (c16)
-                    clr16[t * NC + cell] = 0;
-                else
-                    clr32[t * NC + cell] = 0u;
-            }
-        }
+        if (t < nt && upd) W[t * NC + cell] = w[t];
     }
     return ef;
 }
@@ -800,13 +790,13 @@ __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, fl
 // counts, n_cells and the tile start multiples of 4).
 template <int NT, bool FUSED>
 __device__ __forceinline__ double field_cells4(int64_t cell, int64_t NC, float scale, bool lit, bool upd,
-                                               const uint32_t* src32, uint32_t* clr32, float* W, const float* cf,
+                                               const uint32_t* src32, float* W, const float* cf,
                                                unsigned long long* avg) {
     uint4 cv[NT];
     float4 wv[NT];
 #pragma unroll
     for (int u = 0; u < NT; ++u) {
-        cv[u] = __ldcs(reinterpret_cast<const uint4*>(src32 + u * NC + cell));
+        cv[u] = *reinterpret_cast<const uint4*>(src32 + u * NC + cell);
         if (!upd) wv[u] = *reinterpret_cast<const float4*>(W + u * NC + cell);
     }
     if (avg) {
@@ -842,7 +832,6 @@ __device__ __forceinline__ double field_cells4(int64_t cell, int64_t NC, float s
 #pragma unroll
     for (int u = 0; u < NT; ++u) {
         if (upd) *reinterpret_cast<float4*>(W + u * NC + cell) = wv[u];
-        if (FUSED) *reinterpret_cast<uint4*>(clr32 + u * NC + cell) = make_uint4(0u, 0u, 0u, 0u);
     }
     return ef;
 }
@@ -915,8 +904,7 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
         const float scale = S->scale;
         const bool lit = S->hamiltonian == 1;
         const bool c16 = S->count16 != 0;
-        const uint32_t* src32 = S->counts[FUSED ? (cur ^ 1u) : cur];
-        uint32_t* clr32 = FUSED ? S->counts[cur] : nullptr;
+        const uint32_t* src32 = S->counts[cur];
         float* W = S->omega;
         // the fused sweep samples the time-averaged density at every avg_every-th sweep
         unsigned long long* avg = FUSED && S->avg && S->avg_every && (sweep % S->avg_every) == 0u ? S->avg : nullptr;
@@ -924,10 +912,10 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
         const int64_t end = t.cell0 + t.n_cells;
         if (NT > 0 && !c16 && (NC & 3) == 0 && (t.cell0 & 3) == 0 && (t.n_cells & 3) == 0) {
             for (int64_t cell = t.cell0 + 4 * tid; cell < end; cell += 4 * T)
-                ef += field_cells4<(NT > 0 ? NT : 1), FUSED>(cell, NC, scale, lit, upd, src32, clr32, W, cf, avg);
+                ef += field_cells4<(NT > 0 ? NT : 1), FUSED>(cell, NC, scale, lit, upd, src32, W, cf, avg);
         } else {
             for (int64_t cell = t.cell0 + tid; cell < end; cell += T)
-                ef += field_cell<NT, FUSED>(n, cell, NC, scale, lit, upd, c16, src32, clr32, W, cf, avg);
+                ef += field_cell<NT, FUSED>(n, cell, NC, scale, lit, upd, c16, src32, W, cf, avg);
         }
         ef = warp_sum(ef);
         if (lane == 0) s_ef[warp] = ef;
@@ -1427,8 +1415,8 @@ __global__ void __launch_bounds__(256) k_field_noalloc(const uint32_t* __restric
     const int64_t c1 = min(c0 + (int64_t)kNoAllocTileCells, p.n_cells);
     double ef = 0.0;
     for (int64_t cell = c0 + tid; cell < c1; cell += T)
-        ef += field_cell<0, false>(p.n_types, cell, p.n_cells, p.scale, p.lit != 0, true, false, counts, nullptr,
-                                   omega, cf, nullptr);
+        ef += field_cell<0, false>(p.n_types, cell, p.n_cells, p.scale, p.lit != 0, true, false, counts, omega, cf,
+                                   nullptr);
     ef = warp_sum(ef);
     if (lane == 0) s_ef[warp] = ef;
     __syncthreads();
