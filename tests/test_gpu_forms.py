@@ -264,3 +264,25 @@ def test_server_destroy_cancels_outstanding_work(nb):
     t0 = time.time()
     srv.close()
     assert time.time() - t0 < 10
+
+
+def test_bench_line_contract():
+    """A short plain-form bench run prints one JSON line with every key of the
+    benchmark contract, a roofline of the move kernel and sampled clocks."""
+    import json
+    import sys
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--forms", "plain", "--steps", "3", "--warmup",
+                        "3", "--no-cpu-baseline"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.strip().startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "roofline", "e2e", "clocks", "gpu_launches"):
+        assert k in d, k
+    assert d["steps"] == 3 and d["warmup"] == 3 and d["value"] > 0 and d["gpu_launches"] == 6
+    rf = d["roofline"]
+    assert rf["bound"] == "hbm" and rf["unit"] == "GB/s" and 0 < rf["frac"] < 1.5
+    assert abs(rf["frac"] - rf["achieved"] / rf["peak"]) < 1e-9
+    assert d["e2e"]["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] > 0 and d["e2e"]["d2h_bytes_per_step"] > 0
+    assert "workload" in d["config"]
