@@ -218,6 +218,18 @@ void field_coefficients(int n, const double* xn, int nref, int hamiltonian, floa
 
 // 0: every axis a power of two (the move kernels may compile only the mask
 // fold), 1: some axis is not.
+int flat_threads_for(int tpc, int threads_move) {
+    // lcm(tpc, 32): a block of that many threads holds whole chains with no idle lane
+    int a = tpc, b = 32;
+    while (b) {
+        const int r = a % b;
+        a = b;
+        b = r;
+    }
+    const int l = tpc / a * 32;
+    return l <= 256 ? l : std::max(32, threads_move);
+}
+
 int fold_kind_of(const scmf_spec& s) {
     const int dims[3] = {s.nx, s.ny, s.nz};
     bool pow2 = true;
@@ -318,6 +330,7 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t, cudaStream_t st) 
     max_chains = p.max_chains;
     linear = p.linear;
     fold_kind = p.fold_kind;
+    flat_threads = p.flat_threads > 0 ? p.flat_threads : t.threads_move;
     n_sys = (int)p.close.size();
     std::vector<int32_t> fl, wl;
     for (size_t i = 0; i < p.move.size(); ++i) (p.tile_flat[i] ? fl : wl).push_back((int32_t)i);
@@ -361,6 +374,7 @@ LaunchShape DevPlan::move_shape() const {
     sh.warp_list = d_warp_list;
     sh.n_warp = n_warp;
     sh.fold = fold_kind;
+    sh.flat_threads = flat_threads;
     return sh;
 }
 
@@ -454,7 +468,7 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
             // iteration, and a tile that is not a multiple of cpi ends on a mostly
             // idle one (measured 2.5 % on the large system)
             const int tpc = (A.length + 1) / 2;
-            const int threads = std::max(32, t.threads_move);
+            const int threads = 32 % tpc ? flat_threads_for(tpc, t.threads_move) : std::max(32, t.threads_move);
             const int cpi = 32 % tpc ? std::max(1, threads / tpc) : (32 / tpc) * (threads / 32);
             cpt = std::max(cpi, (cpt + cpi / 2) / cpi * cpi);
         }
@@ -469,7 +483,12 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
             mt.n_tiles_sys = 0;
             mt.arch_index = (int32_t)a;
             p->move.push_back(mt);
-            p->tile_flat.push_back(A.linear && A.length <= 64 && 32 % ((A.length + 1) / 2) != 0 ? 1 : 0);
+            const bool flat = A.linear && A.length <= 64 && 32 % ((A.length + 1) / 2) != 0;
+            p->tile_flat.push_back(flat ? 1 : 0);
+            if (flat) {
+                const int ft = flat_threads_for((A.length + 1) / 2, t.threads_move);
+                p->flat_threads = p->flat_threads == 0 || p->flat_threads == ft ? ft : -1;  // -1: archs disagree
+            }
             p->max_tile_beads = std::max(p->max_tile_beads, mt.n_chains * A.length);
             p->max_chains = std::max(p->max_chains, mt.n_chains);
         }

@@ -54,6 +54,9 @@ uint32_t magic_for(uint32_t n);
 size_t system_device_bytes(const scmf_spec& s);
 void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d);
 int fold_kind_of(const scmf_spec& s);  // 0: every grid axis a power of two, 1: otherwise
+// Block size for chains of ceil(L/2) = tpc threads laid across warps:
+// lcm(tpc, 32) when it is at most 256 (no idle lane), else threads_move.
+int flat_threads_for(int tpc, int threads_move);
 
 // Work decomposition of one or many systems for one launch shape.
 struct Plan {
@@ -67,6 +70,7 @@ struct Plan {
     int max_chains = 0;   // most chains in one move tile
     bool linear = true;
     int fold_kind = 0;  // largest fold_kind_of() of the systems
+    int flat_threads = 0;  // block size of the block-wide move launch (0: none yet, -1: archs disagree)
     std::vector<uint8_t> tile_flat;  // per move tile: chains run across warps (32 % ceil(L/2) != 0)
 };
 
@@ -84,6 +88,7 @@ struct DevPlan {
     int32_t* d_warp_list = nullptr;  // tile indices for the warp-wise register kernel
     int n_flat = 0, n_warp = 0;
     int fold_kind = 0;
+    int flat_threads = 0;
     scmf_tune tune{};
     cudaGraphExec_t graph = nullptr;
     cudaGraph_t graph_src = nullptr;

@@ -163,6 +163,7 @@ struct LaunchShape {
     int n_warp;
     int part;        // 0: every tile; 1: warp tiles only; 2: flat tiles only
     int fold;        // 0: every system's grid axes are powers of two (mask-only fold)
+    int flat_threads;  // block size of the block-wide launch (0: threads)
 };
 
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);

@@ -1268,8 +1268,9 @@ static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, L
             launch_reg<MODE, false>(sh.fold, sh.blocks > 0 ? min(sh.blocks, n_warp) : n_warp, sh.threads, st, tiles,
                                     warp_list, n_warp, acc);
         if (sh.n_flat > 0 && sh.part != 1)
-            launch_reg<MODE, true>(sh.fold, sh.blocks > 0 ? min(sh.blocks, sh.n_flat) : sh.n_flat, sh.threads, st,
-                                   tiles, sh.flat_list, sh.n_flat, acc);
+            launch_reg<MODE, true>(sh.fold, sh.blocks > 0 ? min(sh.blocks, sh.n_flat) : sh.n_flat,
+                                   sh.flat_threads > 0 ? sh.flat_threads : sh.threads, st, tiles, sh.flat_list,
+                                   sh.n_flat, acc);
     } else if (sh.linear) {
         // per-warp slice: ceil(chains per tile / warps) chains of the longest length
         const int nw = sh.threads / 32;
