@@ -74,7 +74,8 @@ __global__ void k_init_coords(SysDev* __restrict__ S, const ArchDev* __restrict_
 struct MoveConsts {
     float k, k2, A, R, inv_dx, inv_dy, inv_dz;
     int nx, ny, nz;
-    bool pow2;  // every axis a power of two
+    bool pow2;   // every axis a power of two
+    bool small;  // every axis of 2 to 256 cells (fold_magic)
 };
 
 __device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
@@ -82,7 +83,13 @@ __device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
 __device__ __forceinline__ void load_fold(MoveConsts& c, const SysDev* S) {
     c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
     c.pow2 = is_pow2(c.nx) && is_pow2(c.ny) && is_pow2(c.nz);
+    c.small = c.nx >= 2 && c.ny >= 2 && c.nz >= 2 && c.nx <= 256 && c.ny <= 256 && c.nz <= 256;
 }
+
+// Offsets and magic multipliers of fold_magic for n = 0 .. 256 (filled once
+// per device by configure_kernels).  Every lane of a warp reads the entry of
+// the same n, which the constant cache broadcasts.
+__constant__ int2 c_fold[257];
 
 // FOLD = 0: every system of the launch has power-of-two axes, so only the
 // mask fold is compiled in; FOLD = -1 picks the fold per system at run time.
@@ -93,6 +100,11 @@ __device__ __forceinline__ int cell_of(const MoveConsts& c, float x, float y, fl
         ix = fold_pow2(x, c.inv_dx, c.nx - 1);
         iy = fold_pow2(y, c.inv_dy, c.ny - 1);
         iz = fold_pow2(z, c.inv_dz, c.nz - 1);
+    } else if (c.small) {
+        const int2 fx = c_fold[c.nx], fy = c_fold[c.ny], fz = c_fold[c.nz];
+        ix = fold_magic(x, c.inv_dx, c.nx, fx.x, (uint32_t)fx.y);
+        iy = fold_magic(y, c.inv_dy, c.ny, fy.x, (uint32_t)fy.y);
+        iz = fold_magic(z, c.inv_dz, c.nz, fz.x, (uint32_t)fz.y);
     } else {
         ix = fold(x, c.inv_dx, c.nx);
         iy = fold(y, c.inv_dy, c.ny);
@@ -1229,8 +1241,21 @@ static cudaError_t allow_smem(int bytes) {
 }
 
 int configure_kernels() {
-    static int done = 0;
-    if (done) return 0;
+    // once per device, with that device current
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    cudaError_t e0 = cudaGetDevice(&dev);
+    if (e0 != cudaSuccess) return (int)e0;
+    std::lock_guard<std::mutex> g(mu);
+    if (dev >= 0 && dev < 64 && done[dev]) return 0;
+    int2 fold_tab[257] = {};
+    for (uint32_t n = 2; n <= 256; ++n) {
+        const uint32_t bias = n * (((1u << 22) + n - 1) / n);  // a multiple of n, at least 2^22
+        fold_tab[n] = make_int2((int)(0x4B400000u - bias), (int)(uint32_t)(((1ull << 32) + n - 1) / n));
+    }
+    cudaError_t ef = cudaMemcpyToSymbol(c_fold, fold_tab, sizeof fold_tab);
+    if (ef != cudaSuccess) return (int)ef;
     const int bytes = (int)sweep_smem_bytes(kMaxTileBeads, kMaxLength);
     cudaError_t e = allow_smem<kMoveOnly, false>(bytes);
     if (e == cudaSuccess) e = allow_smem<kMoveGrid, false>(bytes);
@@ -1241,7 +1266,7 @@ int configure_kernels() {
         e = cudaFuncSetAttribute(k_sweep_linear<kMoveGrid>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_sweep_linear<kGridOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) done = 1;
+    if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return (int)e;
 }
 

@@ -166,6 +166,20 @@ __device__ __forceinline__ int fold(float x, float inv_d, int n) {
     return i;
 }
 
+// The same fold for 2 <= n <= 256 without selects or branches.  The floor is
+// read with a bias B = n * ceil(2^22 / n) folded into the integer offset
+// (off = 0x4B400000 - B), so j = floor(t) + B lies in [0, 2^23 + n) for
+// |t| < 2^22, and j mod n = j - n * umulhi(j, mag) with mag = ceil(2^32 / n),
+// exact for every j < 2^24 and n <= 256 (Granlund and Montgomery, "Division
+// by invariant integers using multiplication", PLDI 1994; checked for all
+// such j and n).  Clamping j below 2^24 keeps every input, NaN included,
+// inside [0, n).  off and mag come from a table indexed by n.
+__device__ __forceinline__ int fold_magic(float x, float inv_d, int n, int off, uint32_t mag) {
+    uint32_t j = (uint32_t)(__float_as_int(__fadd_rd(__fmul_rn(x, inv_d), 0x1.8p23f)) - off);
+    j = min(j, 0x00FFFFFFu);
+    return (int)(j - __umulhi(j, mag) * (uint32_t)n);
+}
+
 // The same fold for a power-of-two n: the low log2(n) bits of the mantissa
 // of t + 1.5*2^23 (rounded down) are floor(t) mod n, because 0x4B400000, the
 // offset of that mantissa, has no bits below 2^22.  Exact for |t| < 2^22.

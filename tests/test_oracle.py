@@ -196,3 +196,20 @@ def test_scmf0_mean_omega_matches_reference_density_files():
         a, b, c = d["mean_omega"]
         assert a == pytest.approx(c, abs=1e-5) and a == pytest.approx(-b / 2, abs=2e-5)
     assert w == pytest.approx(scmf0_reference([0.125, 0.75, 0.125], xn, 32), abs=1e-6)
+
+
+def test_multiply_high_fold_identity():
+    """The device's branch-free fold for grid axes of 2 to 256 cells: with
+    bias B = n * ceil(2^22 / n) and mag = ceil(2^32 / n), j = floor(t) + B and
+    j - n * umulhi(j, mag) is floor(t) mod n.  Checked here in integers over
+    every n, all small |floor(t)| and the ends of the valid range."""
+    rng = np.random.default_rng(5)
+    for n in range(2, 257):
+        bias = n * (((1 << 22) + n - 1) // n)
+        mag = np.uint64(((1 << 32) + n - 1) // n)
+        fl = np.concatenate([np.arange(-3 * n, 3 * n), np.arange(-(1 << 22), -(1 << 22) + 2 * n),
+                             np.arange((1 << 22) - 2 * n, 1 << 22), rng.integers(-(1 << 22), 1 << 22, 2000)])
+        j = (fl + bias).astype(np.uint64)
+        assert j.min() >= 0 and j.max() < (1 << 24)
+        got = (j - ((j * mag) >> np.uint64(32)) * np.uint64(n)).astype(np.int64)
+        assert np.array_equal(got, np.mod(fl, n)), n
