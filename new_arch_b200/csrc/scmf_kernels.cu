@@ -150,13 +150,18 @@ __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, flo
     const int c_new = cell_of<FOLD>(c, px, py, pz);
     const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + c_new), __ldg(w_t + c_old)), deb);
     // log(u) >= -23 ln2 > -17 for every u the generator yields: dE >= 17 rejects
+    // without the logarithm.  Below that, log_f(u) >= log_floor(u) for every
+    // such u, so -dE <= log_floor(u) rejects without it too (same outcome).
     bool acc;
-    if (dE < 0.0f)
+    if (dE < 0.0f) {
         acc = true;
-    else if (dE < 17.0f)
-        acc = log_f(u01(aw)) < -dE;
-    else
+    } else if (dE < 17.0f) {
+        const float u = u01(aw);
         acc = false;
+        if (-dE > log_floor(u)) acc = log_f(u) < -dE;
+    } else {
+        acc = false;
+    }
     cell_old = c_old;
     cell_new = c_new;
     return acc;

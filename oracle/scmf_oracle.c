@@ -64,6 +64,25 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
 /* Uniform in (0, 1] from bits 9..31: 2 - 1.m with the 23 bits as mantissa. */
 float orc_u01(uint32_t w) { return 2.0f - u2f(0x3F800000u | (w >> 9)); }
 
+/* Test helper for the kernels' early Metropolis reject: over all 2^23 values
+ * orc_u01 yields, counts those whose orc_logf lies below the exponent bound
+ * e * ln2_f - slack (one fma, as the kernel computes it) and returns the
+ * smallest margin log - bound in *min_margin. */
+long orc_log_floor_violations(float ln2_f, float slack, float* min_margin) {
+    long bad = 0;
+    float mm = 1e30f;
+    for (uint32_t j = 0; j < (1u << 23); ++j) {
+        const float u = orc_u01(j << 9);
+        const int e = (int)(f2u(u) >> 23) - 127;
+        const float lo = fmaf((float)e, ln2_f, -slack);
+        const float l = orc_logf(u);
+        if (!(l >= lo)) ++bad;
+        if (l - lo < mm) mm = l - lo;
+    }
+    *min_margin = mm;
+    return bad;
+}
+
 /* Natural log for normal positive floats: x = 2^e m, m in [sqrt(1/2), sqrt(2)),
  * log m = log1p(t) = t + t^2 Q(t), t = m - 1 (exact), Q of degree 8 fitted by
  * weighted least squares on Chebyshev nodes (new_arch_b200/csrc/gen_log_poly.py);

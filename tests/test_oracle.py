@@ -198,6 +198,23 @@ def test_scmf0_mean_omega_matches_reference_density_files():
     assert w == pytest.approx(scmf0_reference([0.125, 0.75, 0.125], xn, 32), abs=1e-6)
 
 
+def test_log_floor_bounds_every_uniform():
+    """The kernels reject a move without the logarithm when -dE <= e ln2 -
+    slack (u in [2^e, 2^(e+1))).  That gives the oracle's outcome only if the
+    bound lies at or below log_f(u) for every u the generator yields: checked
+    over all 2^23 of them with the constants of the device source."""
+    import ctypes as C
+    import re
+    src = open(os.path.join(os.path.dirname(GOLDEN), "..", "new_arch_b200", "csrc", "scmf_math.cuh")).read()
+    m = re.search(r"log_floor\(float u\).*?__fmaf_rn\(__int2float_rn\(e\), ([0-9a-fx.p+-]+)f, -([0-9a-fx.p+-]+)f\)", src, re.S)
+    assert m, "log_floor not found"
+    ln2_f, slack = float.fromhex(m.group(1)), float.fromhex(m.group(2))
+    mm = C.c_float()
+    bad = orc.lib().orc_log_floor_violations(ln2_f, slack, C.byref(mm))
+    assert bad == 0
+    assert 0.0 < mm.value < 2 * slack  # tight enough to skip most logarithms
+
+
 def test_multiply_high_fold_identity():
     """The device's branch-free fold for grid axes of 2 to 256 cells: with
     bias B = n * ceil(2^22 / n) and mag = ceil(2^32 / n), j = floor(t) + B and
