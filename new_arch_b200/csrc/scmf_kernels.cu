@@ -156,9 +156,7 @@ __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, flo
     if (dE < 0.0f) {
         acc = true;
     } else if (dE < 17.0f) {
-        const float u = u01(aw);
-        acc = false;
-        if (-dE > log_floor(u)) acc = log_f(u) < -dE;
+        acc = -dE > log_floor(u01(aw)) && log_f(u01(aw)) < -dE;  // u recomputed: no register held across
     } else {
         acc = false;
     }
