@@ -331,6 +331,8 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t, cudaStream_t st) 
     linear = p.linear;
     fold_kind = p.fold_kind;
     flat_threads = p.flat_threads > 0 ? p.flat_threads : t.threads_move;
+    one_seed = p.one_seed && !p.close.empty();
+    seed = p.seed;
     n_sys = (int)p.close.size();
     std::vector<int32_t> fl, wl;
     for (size_t i = 0; i < p.move.size(); ++i) (p.tile_flat[i] ? fl : wl).push_back((int32_t)i);
@@ -375,6 +377,8 @@ LaunchShape DevPlan::move_shape() const {
     sh.n_warp = n_warp;
     sh.fold = fold_kind;
     sh.flat_threads = flat_threads;
+    sh.keyed = one_seed ? 1 : 0;
+    sh.keys = philox_schedule((uint32_t)seed, (uint32_t)(seed >> 32));
     return sh;
 }
 
@@ -454,6 +458,8 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
     const size_t first_tile = p->move.size();
     const size_t first_field = p->field.size();
     p->fold_kind = std::max(p->fold_kind, fold_kind_of(spec));
+    if (p->close.empty()) p->seed = spec.p.seed;
+    else if (p->seed != spec.p.seed) p->one_seed = false;
     for (size_t a = 0; a < archs.size(); ++a) {
         const ArchHost& A = archs[a];
         if (A.n_chains == 0) continue;

@@ -72,6 +72,8 @@ struct Plan {
     int fold_kind = 0;  // largest fold_kind_of() of the systems
     int flat_threads = 0;  // block size of the block-wide move launch (0: none yet, -1: archs disagree)
     std::vector<uint8_t> tile_flat;  // per move tile: chains run across warps (32 % ceil(L/2) != 0)
+    uint64_t seed = 0;      // the systems' seed when they all share one
+    bool one_seed = true;   // every system appended so far has `seed`
 };
 
 struct DevPlan {
@@ -89,6 +91,8 @@ struct DevPlan {
     int n_flat = 0, n_warp = 0;
     int fold_kind = 0;
     int flat_threads = 0;
+    bool one_seed = false;     // every system of the plan has `seed`: move launches take its key schedule
+    uint64_t seed = 0;
     scmf_tune tune{};
     cudaGraphExec_t graph = nullptr;
     cudaGraph_t graph_src = nullptr;

@@ -147,6 +147,25 @@ struct SysClose {
 };
 
 // Launchers (scmf_kernels.cu).  Every pointer is device memory.
+// Round keys of Philox4x32-10 for one 64-bit key: round r XORs in
+// (k0 + r * 0x9E3779B9, k1 + r * 0xBB67AE85) (mod 2^32).  Passed to a kernel
+// by value, the schedule sits in the parameter constant bank, so each round's
+// XOR reads its key there instead of advancing two key registers.
+struct PhiloxKeys {
+    uint32_t k[20];  // k[2r], k[2r + 1]: the two key words of round r
+};
+
+inline PhiloxKeys philox_schedule(uint32_t k0, uint32_t k1) {
+    PhiloxKeys s;
+    for (int r = 0; r < 10; ++r) {
+        s.k[2 * r] = k0;
+        s.k[2 * r + 1] = k1;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return s;
+}
+
 struct LaunchShape {
     int blocks;    // 0 = one CTA per tile
     int threads;
@@ -164,6 +183,8 @@ struct LaunchShape {
     int part;        // 0: every tile; 1: warp tiles only; 2: flat tiles only
     int fold;        // 0: every system's grid axes are powers of two (mask-only fold)
     int flat_threads;  // block size of the block-wide launch (0: threads)
+    int keyed;       // sweep kernel: every system of the launch has the seed of `keys`
+    PhiloxKeys keys;
 };
 
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);

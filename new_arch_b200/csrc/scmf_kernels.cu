@@ -560,10 +560,14 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
 #ifndef SCMF_REG_MIN_BLOCKS
 #define SCMF_REG_MIN_BLOCKS 3
 #endif
-template <int MODE, bool ANY_FLAT, int FOLD>
+// KEYED: every system of the launch has the seed whose Philox round keys are
+// in `keys` (a kernel parameter); otherwise each tile's system key is read
+// from its SysDev and advanced round by round.
+template <int MODE, bool ANY_FLAT, int FOLD, bool KEYED>
 __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const MoveTile* __restrict__ tiles,
                                                                         const int32_t* __restrict__ list, int n_list,
-                                                                        unsigned* __restrict__ acc_part) {
+                                                                        unsigned* __restrict__ acc_part,
+                                                                        const PhiloxKeys keys) {
     // even bead of each warp's lane 0 after its move, double-buffered by
     // iteration parity: with one barrier per iteration a warp may write the
     // next iteration's slot while its left neighbour still reads this one
@@ -656,7 +660,8 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     int deg = 0;
                     if (tt > 0) { qx[0] = lx; qy[0] = ly; qz[0] = lz; deg = 1; }
                     if (has_o) { qx[deg] = xo; qy[deg] = yo; qz[deg] = zo; ++deg; }
-                    const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1);
+                    const uint4 w = KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), keys)
+                                          : philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1);
                     float n0, n1, n2;
                     normals3_spare(w, n0, n1, n2, spare);
                     float px, py, pz;
@@ -694,7 +699,8 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     qx[0] = xe; qy[0] = ye; qz[0] = ze;
                     int deg = 1;
                     if (bo + 1 < L) { qx[1] = rx; qy[1] = ry; qz[1] = rz; deg = 2; }
-                    const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1);
+                    const uint4 w = KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys)
+                                          : philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1);
                     float n0, n1, n2;
                     normals3_odd(spare, w, n0, n1, n2);
                     float px, py, pz;
@@ -1274,12 +1280,19 @@ int configure_kernels() {
 }
 
 template <int MODE, bool FLAT>
-static void launch_reg(int fold, int blocks, int threads, cudaStream_t st, const MoveTile* tiles, const int32_t* list,
-                       int n, unsigned* acc) {
-    if (fold == 0)
-        k_sweep_reg<MODE, FLAT, 0><<<blocks, threads, 0, st>>>(tiles, list, n, acc);
-    else
-        k_sweep_reg<MODE, FLAT, -1><<<blocks, threads, 0, st>>>(tiles, list, n, acc);
+static void launch_reg(const LaunchShape& sh, int blocks, int threads, cudaStream_t st, const MoveTile* tiles,
+                       const int32_t* list, int n, unsigned* acc) {
+    if (MODE != kGridOnly && sh.keyed) {
+        if (sh.fold == 0)
+            k_sweep_reg<MODE, FLAT, 0, true><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
+        else
+            k_sweep_reg<MODE, FLAT, -1, true><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
+    } else {
+        if (sh.fold == 0)
+            k_sweep_reg<MODE, FLAT, 0, false><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
+        else
+            k_sweep_reg<MODE, FLAT, -1, false><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
+    }
 }
 
 template <int MODE>
@@ -1293,10 +1306,10 @@ static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, L
         const int n_warp = sh.n_flat > 0 ? sh.n_warp : n_tiles;
         const int32_t* warp_list = sh.n_flat > 0 ? sh.warp_list : nullptr;
         if (n_warp > 0 && sh.part != 2)
-            launch_reg<MODE, false>(sh.fold, sh.blocks > 0 ? min(sh.blocks, n_warp) : n_warp, sh.threads, st, tiles,
+            launch_reg<MODE, false>(sh, sh.blocks > 0 ? min(sh.blocks, n_warp) : n_warp, sh.threads, st, tiles,
                                     warp_list, n_warp, acc);
         if (sh.n_flat > 0 && sh.part != 1)
-            launch_reg<MODE, true>(sh.fold, sh.blocks > 0 ? min(sh.blocks, sh.n_flat) : sh.n_flat,
+            launch_reg<MODE, true>(sh, sh.blocks > 0 ? min(sh.blocks, sh.n_flat) : sh.n_flat,
                                    sh.flat_threads > 0 ? sh.flat_threads : sh.threads, st, tiles, sh.flat_list,
                                    sh.n_flat, acc);
     } else if (sh.linear) {

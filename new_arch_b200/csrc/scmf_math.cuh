@@ -15,6 +15,8 @@
 #pragma once
 #include <stdint.h>
 
+#include "scmf_internal.h"
+
 namespace scmf {
 
 // Philox4x32-10: Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
@@ -29,6 +31,19 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
         c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1, (uint32_t)p0);
         k0 += 0x9E3779B9u;
         k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// philox4x32_10 with the round keys taken from a schedule (PhiloxKeys, the
+// same bits).
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, const PhiloxKeys& ks) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+        c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ ks.k[2 * r], (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ ks.k[2 * r + 1],
+                       (uint32_t)p0);
     }
     return c;
 }
