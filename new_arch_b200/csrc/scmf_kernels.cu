@@ -114,29 +114,27 @@ __device__ __forceinline__ int cell_of(const MoveConsts& c, float x, float y, fl
 }
 
 
-// One smart-MC trial (device_function.cu:637-717, 562-588, 444-454) of a bead
-// at (x,y,z) with deg bonded neighbours q[0..deg) in ascending bead order.
-// With f = 2k sum_j (q_j - p) the force and d = A f + R xi the displacement,
-// the reference's bonded energy change plus smart-MC correction equals
-// (A c / 4)(c |d|^2 - 2 f.d), c = 2k deg (the force at p + d is f - c d).
-// Same FP32 expression (explicit fma) as the oracle's move_bead().  Returns
-// whether the move is accepted; (px,py,pz) is the final position and cell the
-// final cell index.
-template <int MAXDEG, int FOLD = -1>
-__device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, float z, const float* qx,
-                                      const float* qy, const float* qz, int deg, float cc, float ac4, float n0,
-                                      float n1, float n2, uint32_t aw, const float* __restrict__ w_t, float& px,
-                                      float& py, float& pz, int& cell_old, int& cell_new) {
-    const float k2 = c.k2, A = c.A, R = c.R;
-    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-#pragma unroll
-    for (int d = 0; d < MAXDEG; ++d) {
-        if (d < deg) {
-            fx = __fmaf_rn(__fsub_rn(qx[d], x), k2, fx);
-            fy = __fmaf_rn(__fsub_rn(qy[d], y), k2, fy);
-            fz = __fmaf_rn(__fsub_rn(qz[d], z), k2, fz);
-        }
-    }
+// Bond force f = 2k sum_j (q_j - p), one neighbour at a time in ascending
+// bead order (fma per neighbour, as the oracle).
+__device__ __forceinline__ void add_bond(float k2, float x, float y, float z, float qx, float qy, float qz, float& fx,
+                                         float& fy, float& fz) {
+    fx = __fmaf_rn(__fsub_rn(qx, x), k2, fx);
+    fy = __fmaf_rn(__fsub_rn(qy, y), k2, fy);
+    fz = __fmaf_rn(__fsub_rn(qz, z), k2, fz);
+}
+
+// The trial of a bead at (x,y,z) with bond force f.  With d = A f + R xi the
+// displacement, the reference's bonded energy change plus smart-MC correction
+// equals (A c / 4)(c |d|^2 - 2 f.d), c = 2k deg (the force at p + d is
+// f - c d).  Same FP32 expression (explicit fma) as the oracle's move_bead().
+// Returns whether the move is accepted; (px,py,pz) is the proposed position
+// and cell_old / cell_new the cells of the old and proposed positions.
+template <int FOLD = -1>
+__device__ __forceinline__ bool trial_f(const MoveConsts& c, float x, float y, float z, float fx, float fy, float fz,
+                                        float cc, float ac4, float n0, float n1, float n2, uint32_t aw,
+                                        const float* __restrict__ w_t, float& px, float& py, float& pz, int& cell_old,
+                                        int& cell_new) {
+    const float A = c.A, R = c.R;
     const float dx = __fmaf_rn(A, fx, __fmul_rn(R, n0));
     const float dy = __fmaf_rn(A, fy, __fmul_rn(R, n1));
     const float dz = __fmaf_rn(A, fz, __fmul_rn(R, n2));
@@ -163,6 +161,20 @@ __device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, flo
     cell_old = c_old;
     cell_new = c_new;
     return acc;
+}
+
+// One smart-MC trial (device_function.cu:637-717, 562-588, 444-454) of a bead
+// at (x,y,z) with deg bonded neighbours q[0..deg) in ascending bead order.
+template <int MAXDEG, int FOLD = -1>
+__device__ __forceinline__ bool trial(const MoveConsts& c, float x, float y, float z, const float* qx,
+                                      const float* qy, const float* qz, int deg, float cc, float ac4, float n0,
+                                      float n1, float n2, uint32_t aw, const float* __restrict__ w_t, float& px,
+                                      float& py, float& pz, int& cell_old, int& cell_new) {
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+#pragma unroll
+    for (int d = 0; d < MAXDEG; ++d)
+        if (d < deg) add_bond(c.k2, x, y, z, qx[d], qy[d], qz[d], fx, fy, fz);
+    return trial_f<FOLD>(c, x, y, z, fx, fy, fz, cc, ac4, n0, n1, n2, aw, w_t, px, py, pz, cell_old, cell_new);
 }
 
 // Counts are kept as the grid of the current positions: a fused sweep moves
@@ -656,19 +668,36 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     lz = __ldcg(S->z + g - 1);
                 }
                 if (live) {
+                    // neighbours in ascending bead order: 2t-1 (if any), then 2t+1 (if any).
+                    // The keyed mask-fold instance adds their forces one at a time and then
+                    // keeps no local array and no spill; the other instances spill 16-32 B
+                    // that way and take them through a two-entry array instead (in a 24 B
+                    // stack frame).  Same fma sequence either way.
+                    constexpr bool one_by_one = KEYED && FOLD == 0;
+                    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
                     float qx[2], qy[2], qz[2];
                     int deg = 0;
-                    if (tt > 0) { qx[0] = lx; qy[0] = ly; qz[0] = lz; deg = 1; }
-                    if (has_o) { qx[deg] = xo; qy[deg] = yo; qz[deg] = zo; ++deg; }
+                    if (one_by_one) {
+                        if (tt > 0) add_bond(c.k2, xe, ye, ze, lx, ly, lz, fx, fy, fz);
+                        if (has_o) add_bond(c.k2, xe, ye, ze, xo, yo, zo, fx, fy, fz);
+                        deg = (tt > 0 ? 1 : 0) + (has_o ? 1 : 0);
+                    } else {
+                        if (tt > 0) { qx[0] = lx; qy[0] = ly; qz[0] = lz; deg = 1; }
+                        if (has_o) { qx[deg] = xo; qy[deg] = yo; qz[deg] = zo; ++deg; }
+                    }
                     const uint4 w = KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), keys)
                                           : philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1);
                     float n0, n1, n2;
                     normals3_spare(w, n0, n1, n2, spare);
                     float px, py, pz;
                     int c_old, c_new;
-                    const bool acc = trial<2, FOLD>(c, xe, ye, ze, qx, qy, qz, deg, deg == 2 ? cc2 : (deg == 1 ? cc1 : 0.0f),
-                                              deg == 2 ? ac42 : (deg == 1 ? ac41 : 0.0f), n0, n1, n2, accept_word(w),
-                                              omega + (int64_t)type_e * NC, px, py, pz, c_old, c_new);
+                    const float cc = deg == 2 ? cc2 : (deg == 1 ? cc1 : 0.0f);
+                    const float ac4 = deg == 2 ? ac42 : (deg == 1 ? ac41 : 0.0f);
+                    const float* w_e = omega + (int64_t)type_e * NC;
+                    const bool acc = one_by_one ? trial_f<FOLD>(c, xe, ye, ze, fx, fy, fz, cc, ac4, n0, n1, n2,
+                                                               accept_word(w), w_e, px, py, pz, c_old, c_new)
+                                               : trial<2, FOLD>(c, xe, ye, ze, qx, qy, qz, deg, cc, ac4, n0, n1, n2,
+                                                                accept_word(w), w_e, px, py, pz, c_old, c_new);
                     if (acc) { xe = px; ye = py; ze = pz; }
                     nacc += acc ? 1u : 0u;
                     if (MODE == kMoveGrid && acc && c_new != c_old)
