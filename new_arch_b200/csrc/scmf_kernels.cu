@@ -584,6 +584,12 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
     // iteration parity: with one barrier per iteration a warp may write the
     // next iteration's slot while its left neighbour still reads this one
     __shared__ float s_first_even[2][kMaxWarps][3];
+    // The keyed mask-fold instance has registers to spare once its Philox key
+    // lives in the parameter bank: it adds the even bead's bond forces one at a
+    // time (no local array) and computes the odd bead's Philox block together
+    // with the even bead's (two independent chains of rounds to interleave).
+    // The other instances spill either way; all give the same bits.
+    constexpr bool kLean = KEYED && FOLD == 0;
     int parity = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int li = blockIdx.x; li < n_list; li += gridDim.x) {
@@ -654,6 +660,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                 continue;
             }
             float spare = 0.0f;  // spare sine of the even bead's block, first normal of the odd bead
+            uint32_t wo_x = 0u, wo_y = 0u, wo_a = 0u;  // kLean: the odd bead's words (Box-Muller pair, accept)
             // even half-sweep
             {
                 float lx = __shfl_up_sync(0xffffffffu, xo, 1);
@@ -668,16 +675,13 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     lz = __ldcg(S->z + g - 1);
                 }
                 if (live) {
-                    // neighbours in ascending bead order: 2t-1 (if any), then 2t+1 (if any).
-                    // The keyed mask-fold instance adds their forces one at a time and then
-                    // keeps no local array and no spill; the other instances spill 16-32 B
-                    // that way and take them through a two-entry array instead (in a 24 B
-                    // stack frame).  Same fma sequence either way.
-                    constexpr bool one_by_one = KEYED && FOLD == 0;
+                    // neighbours in ascending bead order: 2t-1 (if any), then 2t+1 (if any),
+                    // one at a time (kLean) or through a two-entry array (in a 24 B stack
+                    // frame; the other instances spill 16-32 B without it).  Same fma sequence.
                     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
                     float qx[2], qy[2], qz[2];
                     int deg = 0;
-                    if (one_by_one) {
+                    if (kLean) {
                         if (tt > 0) add_bond(c.k2, xe, ye, ze, lx, ly, lz, fx, fy, fz);
                         if (has_o) add_bond(c.k2, xe, ye, ze, xo, yo, zo, fx, fy, fz);
                         deg = (tt > 0 ? 1 : 0) + (has_o ? 1 : 0);
@@ -687,6 +691,12 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     }
                     const uint4 w = KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), keys)
                                           : philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1);
+                    if (kLean) {
+                        const uint4 wo = philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys);
+                        wo_x = wo.x;
+                        wo_y = wo.y;
+                        wo_a = accept_word(wo);
+                    }
                     float n0, n1, n2;
                     normals3_spare(w, n0, n1, n2, spare);
                     float px, py, pz;
@@ -694,10 +704,10 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     const float cc = deg == 2 ? cc2 : (deg == 1 ? cc1 : 0.0f);
                     const float ac4 = deg == 2 ? ac42 : (deg == 1 ? ac41 : 0.0f);
                     const float* w_e = omega + (int64_t)type_e * NC;
-                    const bool acc = one_by_one ? trial_f<FOLD>(c, xe, ye, ze, fx, fy, fz, cc, ac4, n0, n1, n2,
-                                                               accept_word(w), w_e, px, py, pz, c_old, c_new)
-                                               : trial<2, FOLD>(c, xe, ye, ze, qx, qy, qz, deg, cc, ac4, n0, n1, n2,
-                                                                accept_word(w), w_e, px, py, pz, c_old, c_new);
+                    const bool acc = kLean ? trial_f<FOLD>(c, xe, ye, ze, fx, fy, fz, cc, ac4, n0, n1, n2,
+                                                           accept_word(w), w_e, px, py, pz, c_old, c_new)
+                                           : trial<2, FOLD>(c, xe, ye, ze, qx, qy, qz, deg, cc, ac4, n0, n1, n2,
+                                                            accept_word(w), w_e, px, py, pz, c_old, c_new);
                     if (acc) { xe = px; ye = py; ze = pz; }
                     nacc += acc ? 1u : 0u;
                     if (MODE == kMoveGrid && acc && c_new != c_old)
@@ -728,14 +738,15 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     qx[0] = xe; qy[0] = ye; qz[0] = ze;
                     int deg = 1;
                     if (bo + 1 < L) { qx[1] = rx; qy[1] = ry; qz[1] = rz; deg = 2; }
-                    const uint4 w = KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys)
-                                          : philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1);
+                    const uint4 w = kLean   ? make_uint4(wo_x, wo_y, 0u, 0u)
+                                    : KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys)
+                                            : philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1);
                     float n0, n1, n2;
                     normals3_odd(spare, w, n0, n1, n2);
                     float px, py, pz;
                     int c_old, c_new;
                     const bool acc = trial<2, FOLD>(c, xo, yo, zo, qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
-                                              deg == 2 ? ac42 : ac41, n0, n1, n2, accept_word(w),
+                                              deg == 2 ? ac42 : ac41, n0, n1, n2, kLean ? wo_a : accept_word(w),
                                               omega + (int64_t)type_o * NC, px, py, pz, c_old, c_new);
                     if (acc) { xo = px; yo = py; zo = pz; }
                     nacc += acc ? 1u : 0u;
