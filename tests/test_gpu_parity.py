@@ -210,6 +210,27 @@ def test_batch_bit_identical_to_alone(nb):
         s.close()
 
 
+def test_same_seed_batch_matches_oracle(nb):
+    """Systems sharing one seed run as one launch with the Philox round keys in
+    the kernel parameters (the instance single systems use); systems with
+    distinct seeds read the key per tile.  Both equal the oracle."""
+    specs = nb.spec.batched_mix(4, mix_seed=11, edge_scale=0.25)
+    for sp in specs:
+        sp.seed = 77
+    systems = [nb.System(sp) for sp in specs]
+    for s in systems:
+        s.init_coords()
+    b = nb.Batch(systems, tune={"threads_move": 128})
+    b.step(4)
+    for i, (sp, s) in enumerate(zip(specs, systems)):
+        orc = oracle_for(sp)
+        orc.step(4)
+        compare_state(s, orc, f"same-seed batch member {i}")
+    b.close()
+    for s in systems:
+        s.close()
+
+
 def test_autotune_keeps_state(nb):
     specs = nb.spec.batched_mix(3, mix_seed=9, edge_scale=0.25)
     systems = [nb.System(sp) for sp in specs]
