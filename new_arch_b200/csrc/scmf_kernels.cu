@@ -584,12 +584,12 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
     // iteration parity: with one barrier per iteration a warp may write the
     // next iteration's slot while its left neighbour still reads this one
     __shared__ float s_first_even[2][kMaxWarps][3];
-    // The keyed mask-fold instance has registers to spare once its Philox key
-    // lives in the parameter bank: it adds the even bead's bond forces one at a
-    // time (no local array) and computes the odd bead's Philox block together
-    // with the even bead's (two independent chains of rounds to interleave).
-    // The other instances spill either way; all give the same bits.
-    constexpr bool kLean = KEYED && FOLD == 0;
+    // Every instance computes the odd bead's Philox block together with the
+    // even bead's (two independent chains of rounds to interleave).  The keyed
+    // instances, whose Philox key lives in the parameter bank, also add the even
+    // bead's bond forces one at a time (no local array); the others spill that
+    // way and keep the two-entry array.  All give the same bits.
+    constexpr bool kLean = KEYED;
     int parity = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int li = blockIdx.x; li < n_list; li += gridDim.x) {
@@ -611,6 +611,8 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
         c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
         load_fold(c, S);
         const int64_t NC = S->n_cells;
+        // counts pointer and width: read here for gridding, and again at each (rare)
+        // count move of the move modes, so that no register holds them across a sweep
         uint32_t* cnt = S->counts[S->cur];
         const bool c16 = S->count16 != 0;
         const float* __restrict__ omega = S->omega;
@@ -660,7 +662,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                 continue;
             }
             float spare = 0.0f;  // spare sine of the even bead's block, first normal of the odd bead
-            uint32_t wo_x = 0u, wo_y = 0u, wo_a = 0u;  // kLean: the odd bead's words (Box-Muller pair, accept)
+            uint32_t wo_x = 0u, wo_y = 0u, wo_a = 0u;  // the odd bead's words (Box-Muller pair, accept)
             // even half-sweep
             {
                 float lx = __shfl_up_sync(0xffffffffu, xo, 1);
@@ -691,8 +693,9 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     }
                     const uint4 w = KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), keys)
                                           : philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1);
-                    if (kLean) {
-                        const uint4 wo = philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys);
+                    {
+                        const uint4 wo = KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys)
+                                               : philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1);
                         wo_x = wo.x;
                         wo_y = wo.y;
                         wo_a = accept_word(wo);
@@ -711,7 +714,7 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     if (acc) { xe = px; ye = py; ze = pz; }
                     nacc += acc ? 1u : 0u;
                     if (MODE == kMoveGrid && acc && c_new != c_old)
-                        count_move(cnt, c16, (int64_t)type_e * NC, c_old, c_new);
+                        count_move(S->counts[S->cur], S->count16 != 0, (int64_t)type_e * NC, c_old, c_new);
                 }
             }
             // odd half-sweep
@@ -738,20 +741,17 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                     qx[0] = xe; qy[0] = ye; qz[0] = ze;
                     int deg = 1;
                     if (bo + 1 < L) { qx[1] = rx; qy[1] = ry; qz[1] = rz; deg = 2; }
-                    const uint4 w = kLean   ? make_uint4(wo_x, wo_y, 0u, 0u)
-                                    : KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys)
-                                            : philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1);
                     float n0, n1, n2;
-                    normals3_odd(spare, w, n0, n1, n2);
+                    normals3_odd(spare, make_uint4(wo_x, wo_y, 0u, 0u), n0, n1, n2);
                     float px, py, pz;
                     int c_old, c_new;
                     const bool acc = trial<2, FOLD>(c, xo, yo, zo, qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
-                                              deg == 2 ? ac42 : ac41, n0, n1, n2, kLean ? wo_a : accept_word(w),
+                                              deg == 2 ? ac42 : ac41, n0, n1, n2, wo_a,
                                               omega + (int64_t)type_o * NC, px, py, pz, c_old, c_new);
                     if (acc) { xo = px; yo = py; zo = pz; }
                     nacc += acc ? 1u : 0u;
                     if (MODE == kMoveGrid && acc && c_new != c_old)
-                        count_move(cnt, c16, (int64_t)type_o * NC, c_old, c_new);
+                        count_move(S->counts[S->cur], S->count16 != 0, (int64_t)type_o * NC, c_old, c_new);
                 }
             }
             if (live) {
