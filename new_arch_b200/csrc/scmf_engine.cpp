@@ -332,6 +332,7 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t, cudaStream_t st) 
     fold_kind = p.fold_kind;
     flat_threads = p.flat_threads > 0 ? p.flat_threads : t.threads_move;
     one_seed = p.one_seed && !p.close.empty();
+    one_seed_hi = p.one_seed_hi && !p.close.empty();
     seed = p.seed;
     n_sys = (int)p.close.size();
     std::vector<int32_t> fl, wl;
@@ -377,7 +378,7 @@ LaunchShape DevPlan::move_shape() const {
     sh.n_warp = n_warp;
     sh.fold = fold_kind;
     sh.flat_threads = flat_threads;
-    sh.keyed = one_seed ? 1 : 0;
+    sh.keyed = one_seed ? kKeysBoth : (one_seed_hi ? kKeysHigh : kKeysNone);
     sh.keys = philox_schedule((uint32_t)seed, (uint32_t)(seed >> 32));
     return sh;
 }
@@ -458,8 +459,12 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
     const size_t first_tile = p->move.size();
     const size_t first_field = p->field.size();
     p->fold_kind = std::max(p->fold_kind, fold_kind_of(spec));
-    if (p->close.empty()) p->seed = spec.p.seed;
-    else if (p->seed != spec.p.seed) p->one_seed = false;
+    if (p->close.empty()) {
+        p->seed = spec.p.seed;
+    } else {
+        if (p->seed != spec.p.seed) p->one_seed = false;
+        if ((p->seed >> 32) != (spec.p.seed >> 32)) p->one_seed_hi = false;
+    }
     for (size_t a = 0; a < archs.size(); ++a) {
         const ArchHost& A = archs[a];
         if (A.n_chains == 0) continue;

@@ -74,6 +74,7 @@ struct Plan {
     std::vector<uint8_t> tile_flat;  // per move tile: chains run across warps (32 % ceil(L/2) != 0)
     uint64_t seed = 0;      // the systems' seed when they all share one
     bool one_seed = true;   // every system appended so far has `seed`
+    bool one_seed_hi = true;  // ... or at least its upper 32 bits
 };
 
 struct DevPlan {
@@ -92,6 +93,7 @@ struct DevPlan {
     int fold_kind = 0;
     int flat_threads = 0;
     bool one_seed = false;     // every system of the plan has `seed`: move launches take its key schedule
+    bool one_seed_hi = false;  // they share its upper 32 bits: the second key word's schedule
     uint64_t seed = 0;
     scmf_tune tune{};
     cudaGraphExec_t graph = nullptr;

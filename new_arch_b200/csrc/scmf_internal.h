@@ -166,6 +166,8 @@ inline PhiloxKeys philox_schedule(uint32_t k0, uint32_t k1) {
     return s;
 }
 
+enum KeyMode { kKeysNone = 0, kKeysHigh = 1, kKeysBoth = 2 };
+
 struct LaunchShape {
     int blocks;    // 0 = one CTA per tile
     int threads;
@@ -183,7 +185,9 @@ struct LaunchShape {
     int part;        // 0: every tile; 1: warp tiles only; 2: flat tiles only
     int fold;        // 0: every system's grid axes are powers of two (mask-only fold)
     int flat_threads;  // block size of the block-wide launch (0: threads)
-    int keyed;       // sweep kernel: every system of the launch has the seed of `keys`
+    // sweep kernel: kKeysBoth when every system of the launch has the seed of
+    // `keys`, kKeysHigh when they share its upper 32 bits, else kKeysNone
+    int keyed;
     PhiloxKeys keys;
 };
 

@@ -572,10 +572,18 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
 #ifndef SCMF_REG_MIN_BLOCKS
 #define SCMF_REG_MIN_BLOCKS 3
 #endif
-// KEYED: every system of the launch has the seed whose Philox round keys are
-// in `keys` (a kernel parameter); otherwise each tile's system key is read
-// from its SysDev and advanced round by round.
-template <int MODE, bool ANY_FLAT, int FOLD, bool KEYED>
+// KEYS (KeyMode): kKeysBoth when every system of the launch has the seed whose
+// Philox round keys are in `keys` (a kernel parameter); kKeysHigh when they
+// share its upper 32 bits, so that only the first key word is read from the
+// tile's SysDev and advanced round by round; kKeysNone: both are.
+template <int KEYS>
+__device__ __forceinline__ uint4 philox_block(uint4 ctr, uint32_t k0, uint32_t k1, const PhiloxKeys& keys) {
+    if (KEYS == kKeysBoth) return philox4x32_10(ctr, keys);
+    if (KEYS == kKeysHigh) return philox4x32_10(ctr, k0, keys);
+    return philox4x32_10(ctr, k0, k1);
+}
+
+template <int MODE, bool ANY_FLAT, int FOLD, int KEYS>
 __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const MoveTile* __restrict__ tiles,
                                                                         const int32_t* __restrict__ list, int n_list,
                                                                         unsigned* __restrict__ acc_part,
@@ -586,10 +594,10 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
     __shared__ float s_first_even[2][kMaxWarps][3];
     // Every instance computes the odd bead's Philox block together with the
     // even bead's (two independent chains of rounds to interleave).  The keyed
-    // instances, whose Philox key lives in the parameter bank, also add the even
-    // bead's bond forces one at a time (no local array); the others spill that
-    // way and keep the two-entry array.  All give the same bits.
-    constexpr bool kLean = KEYED;
+    // instances, whose Philox key lives (at least half) in the parameter bank,
+    // also add the even bead's bond forces one at a time (no local array); the
+    // others spill that way and keep the two-entry array.  All give the same bits.
+    constexpr bool kLean = KEYS != kKeysNone;
     int parity = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int li = blockIdx.x; li < n_list; li += gridDim.x) {
@@ -691,11 +699,9 @@ __global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const Mo
                         if (tt > 0) { qx[0] = lx; qy[0] = ly; qz[0] = lz; deg = 1; }
                         if (has_o) { qx[deg] = xo; qy[deg] = yo; qz[deg] = zo; ++deg; }
                     }
-                    const uint4 w = KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), keys)
-                                          : philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1);
+                    const uint4 w = philox_block<KEYS>(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1, keys);
                     {
-                        const uint4 wo = KEYED ? philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys)
-                                               : philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1);
+                        const uint4 wo = philox_block<KEYS>(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1, keys);
                         wo_x = wo.x;
                         wo_y = wo.y;
                         wo_a = accept_word(wo);
@@ -1322,16 +1328,22 @@ int configure_kernels() {
 template <int MODE, bool FLAT>
 static void launch_reg(const LaunchShape& sh, int blocks, int threads, cudaStream_t st, const MoveTile* tiles,
                        const int32_t* list, int n, unsigned* acc) {
-    if (MODE != kGridOnly && sh.keyed) {
+    const int keys = MODE == kGridOnly ? kKeysNone : sh.keyed;
+    if (keys == kKeysBoth) {
         if (sh.fold == 0)
-            k_sweep_reg<MODE, FLAT, 0, true><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
+            k_sweep_reg<MODE, FLAT, 0, kKeysBoth><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
         else
-            k_sweep_reg<MODE, FLAT, -1, true><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
+            k_sweep_reg<MODE, FLAT, -1, kKeysBoth><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
+    } else if (keys == kKeysHigh) {
+        if (sh.fold == 0)
+            k_sweep_reg<MODE, FLAT, 0, kKeysHigh><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
+        else
+            k_sweep_reg<MODE, FLAT, -1, kKeysHigh><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
     } else {
         if (sh.fold == 0)
-            k_sweep_reg<MODE, FLAT, 0, false><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
+            k_sweep_reg<MODE, FLAT, 0, kKeysNone><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
         else
-            k_sweep_reg<MODE, FLAT, -1, false><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
+            k_sweep_reg<MODE, FLAT, -1, kKeysNone><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
     }
 }
 

@@ -48,6 +48,21 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, const PhiloxKeys& ks) {
     return c;
 }
 
+// philox4x32_10 with the first key word advanced in a register and the
+// second word's round keys from a schedule (the same bits): for launches whose
+// systems share the upper 32 bits of their seed.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, const PhiloxKeys& ks) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+        c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ ks.k[2 * r + 1],
+                       (uint32_t)p0);
+        k0 += 0x9E3779B9u;
+    }
+    return c;
+}
+
 // Uniform in (0, 1] from bits 9..31: 2 - 1.m with the 23 bits as mantissa
 // (exact in FP32; no integer-to-float conversion).
 __device__ __forceinline__ float u01(uint32_t w) {

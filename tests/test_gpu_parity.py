@@ -210,13 +210,15 @@ def test_batch_bit_identical_to_alone(nb):
         s.close()
 
 
-def test_same_seed_batch_matches_oracle(nb):
-    """Systems sharing one seed run as one launch with the Philox round keys in
-    the kernel parameters (the instance single systems use); systems with
-    distinct seeds read the key per tile.  Both equal the oracle."""
+@pytest.mark.parametrize("seeds", ["one", "same_high_word", "distinct_high_words"])
+def test_batch_key_modes_match_oracle(nb, seeds):
+    """Systems batched into one launch take their Philox round keys from the
+    kernel parameters when they share a seed, the second key word's only when
+    they share the seed's upper 32 bits, and neither otherwise (each tile's
+    key advanced in registers).  All three launch kinds equal the oracle."""
     specs = nb.spec.batched_mix(4, mix_seed=11, edge_scale=0.25)
-    for sp in specs:
-        sp.seed = 77
+    for i, sp in enumerate(specs):
+        sp.seed = {"one": 77, "same_high_word": 77 + i, "distinct_high_words": 77 + (i << 33)}[seeds]
     systems = [nb.System(sp) for sp in specs]
     for s in systems:
         s.init_coords()
@@ -225,7 +227,7 @@ def test_same_seed_batch_matches_oracle(nb):
     for i, (sp, s) in enumerate(zip(specs, systems)):
         orc = oracle_for(sp)
         orc.step(4)
-        compare_state(s, orc, f"same-seed batch member {i}")
+        compare_state(s, orc, f"{seeds} batch member {i}")
     b.close()
     for s in systems:
         s.close()
