@@ -569,9 +569,6 @@ __global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(con
 // the moved right neighbour through shared memory after one block barrier per
 // iteration; every chain still moves all its even beads before any odd bead.  Tiles are read and written with
 // coalesced float2 accesses.  Same trial and keys as k_sweep.
-#ifndef SCMF_REG_MIN_BLOCKS
-#define SCMF_REG_MIN_BLOCKS 3
-#endif
 // KEYS (KeyMode): kKeysBoth when every system of the launch has the seed whose
 // Philox round keys are in `keys` (a kernel parameter); kKeysHigh when they
 // share its upper 32 bits, so that only the first key word is read from the
@@ -583,8 +580,17 @@ __device__ __forceinline__ uint4 philox_block(uint4 ctr, uint32_t k0, uint32_t k
     return philox4x32_10(ctr, k0, k1);
 }
 
+// Register cap per instance.  80 (six 128-thread CTAs, 24 warps per SM) is
+// what the general instances need without spilling; the instances that read
+// their Philox round keys from the parameter bank fit in 72 without spilling,
+// which gives seven CTAs (28 warps) per SM (large system 0.661 -> 0.621 ms,
+// batched mix +4.4 %).  At 64 (32 warps) they spill 20-36 B.
+constexpr int reg_cap(bool flat, int fold, int keys) {
+    return (keys == kKeysBoth || (keys == kKeysHigh && fold != 0 && !flat)) ? 72 : 80;
+}
+
 template <int MODE, bool ANY_FLAT, int FOLD, int KEYS>
-__global__ void __launch_bounds__(256, SCMF_REG_MIN_BLOCKS) k_sweep_reg(const MoveTile* __restrict__ tiles,
+__global__ void __maxnreg__(reg_cap(ANY_FLAT, FOLD, KEYS)) k_sweep_reg(const MoveTile* __restrict__ tiles,
                                                                         const int32_t* __restrict__ list, int n_list,
                                                                         unsigned* __restrict__ acc_part,
                                                                         const PhiloxKeys keys) {
