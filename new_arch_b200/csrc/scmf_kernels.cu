@@ -227,8 +227,10 @@ size_t sweep_smem_bytes(int max_tile_beads, int max_length) {
 //   counts of the current positions added into counts[cur] (a cleared buffer).
 //   LINEAR: every architecture of the launch is a linear chain (bonds i-i+1,
 //   even beads colour 0, odd beads colour 1); neighbours are computed, not looked up.
+//   Two 256-thread CTAs per SM leave it 128 registers and no spill (at 64 it
+//   spilled ~400 B per thread and moved combs 12 % slower).
 template <int MODE, bool LINEAR>
-__global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ tiles, int n_tiles,
+__global__ void __launch_bounds__(256, 2) k_sweep(const MoveTile* __restrict__ tiles, int n_tiles,
                                                    int max_tile_beads, int max_length, unsigned* __restrict__ acc_part) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sx = reinterpret_cast<float*>(smem_raw);
@@ -403,11 +405,10 @@ __global__ void __launch_bounds__(256, 4) k_sweep(const MoveTile* __restrict__ t
 // so the lanes of a half-sweep read consecutive words, and the warp needs no
 // block barrier: load, even half-sweep, odd half-sweep, store, separated by
 // __syncwarp.  Results are identical to k_sweep (same trial, same keys).
-#ifndef SCMF_SWEEP_MIN_BLOCKS
-#define SCMF_SWEEP_MIN_BLOCKS 4
-#endif
+// Three 256-thread CTAs per SM leave it 80 registers and no spill (at 64 it
+// spilled ~100 B per thread and moved chains of 128 beads 12 % slower).
 template <int MODE>
-__global__ void __launch_bounds__(256, SCMF_SWEEP_MIN_BLOCKS) k_sweep_linear(const MoveTile* __restrict__ tiles,
+__global__ void __launch_bounds__(256, 3) k_sweep_linear(const MoveTile* __restrict__ tiles,
                                                           const int32_t* __restrict__ list, int n_list,
                                                           int warp_beads, unsigned* __restrict__ acc_part) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
