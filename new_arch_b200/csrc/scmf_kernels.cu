@@ -191,13 +191,25 @@ __device__ __forceinline__ void count_move(uint32_t* cnt, bool c16, int64_t typ,
     }
 }
 
+// KEYS (KeyMode): kKeysBoth when every system of the launch has the seed whose
+// Philox round keys are in `keys` (a kernel parameter); kKeysHigh when they
+// share its upper 32 bits, so that only the first key word is read from the
+// tile's SysDev and advanced round by round; kKeysNone: both are.
+template <int KEYS>
+__device__ __forceinline__ uint4 philox_block(uint4 ctr, uint32_t k0, uint32_t k1, const PhiloxKeys& keys) {
+    if (KEYS == kKeysBoth) return philox4x32_10(ctr, keys);
+    if (KEYS == kKeysHigh) return philox4x32_10(ctr, k0, keys);
+    return philox4x32_10(ctr, k0, k1);
+}
+
 // Philox block and normals of bead b of chain gc (odd beads also draw the
 // block of b-1 for its spare sine).
+template <int KEYS>
 __device__ __forceinline__ uint32_t bead_normals(uint32_t gc, int b, uint32_t step, uint32_t k0, uint32_t k1,
-                                                 float& n0, float& n1, float& n2) {
-    const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1);
+                                                 const PhiloxKeys& keys, float& n0, float& n1, float& n2) {
+    const uint4 w = philox_block<KEYS>(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1, keys);
     if (b & 1) {
-        const float sp = spare_of(philox4x32_10(make_uint4(gc, (uint32_t)(b - 1), step, 0u), k0, k1));
+        const float sp = spare_of(philox_block<KEYS>(make_uint4(gc, (uint32_t)(b - 1), step, 0u), k0, k1, keys));
         normals3_odd(sp, w, n0, n1, n2);
     } else {
         normals3(w, n0, n1, n2);
@@ -229,9 +241,10 @@ size_t sweep_smem_bytes(int max_tile_beads, int max_length) {
 //   even beads colour 0, odd beads colour 1); neighbours are computed, not looked up.
 //   Two 256-thread CTAs per SM leave it 128 registers and no spill (at 64 it
 //   spilled ~400 B per thread and moved combs 12 % slower).
-template <int MODE, bool LINEAR>
+template <int MODE, bool LINEAR, int KEYS>
 __global__ void __launch_bounds__(256, 2) k_sweep(const MoveTile* __restrict__ tiles, int n_tiles,
-                                                   int max_tile_beads, int max_length, unsigned* __restrict__ acc_part) {
+                                                   int max_tile_beads, int max_length, unsigned* __restrict__ acc_part,
+                                                   const PhiloxKeys keys) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sx = reinterpret_cast<float*>(smem_raw);
     float* sy = sx + max_tile_beads;
@@ -340,7 +353,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep(const MoveTile* __restrict__ t
                         }
                     }
                     float n0, n1, n2;
-                    const uint32_t aw = bead_normals(__ldg(cid + cl), b, step, k0, k1, n0, n1, n2);
+                    const uint32_t aw = bead_normals<KEYS>(__ldg(cid + cl), b, step, k0, k1, keys, n0, n1, n2);
                     float px, py, pz;
                     int c_old, c_new;
                     const bool acc = trial<LINEAR ? 2 : kMaxDeg>(c, sx[base + b], sy[base + b], sz[base + b], qx, qy,
@@ -407,10 +420,11 @@ __global__ void __launch_bounds__(256, 2) k_sweep(const MoveTile* __restrict__ t
 // __syncwarp.  Results are identical to k_sweep (same trial, same keys).
 // Three 256-thread CTAs per SM leave it 80 registers and no spill (at 64 it
 // spilled ~100 B per thread and moved chains of 128 beads 12 % slower).
-template <int MODE>
+template <int MODE, int KEYS>
 __global__ void __launch_bounds__(256, 3) k_sweep_linear(const MoveTile* __restrict__ tiles,
                                                           const int32_t* __restrict__ list, int n_list,
-                                                          int warp_beads, unsigned* __restrict__ acc_part) {
+                                                          int warp_beads, unsigned* __restrict__ acc_part,
+                                                          const PhiloxKeys keys) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     // per warp: x, y, z of its chains (parity-split), then the spare sine of
@@ -505,7 +519,7 @@ __global__ void __launch_bounds__(256, 3) k_sweep_linear(const MoveTile* __restr
                     }
                     const int type = __ldg(types + b);
                     float n0, n1, n2;
-                    const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1);
+                    const uint4 w = philox_block<KEYS>(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1, keys);
                     if (col == 0) {
                         float sp;
                         normals3_spare(w, n0, n1, n2, sp);
@@ -570,17 +584,6 @@ __global__ void __launch_bounds__(256, 3) k_sweep_linear(const MoveTile* __restr
 // the moved right neighbour through shared memory after one block barrier per
 // iteration; every chain still moves all its even beads before any odd bead.  Tiles are read and written with
 // coalesced float2 accesses.  Same trial and keys as k_sweep.
-// KEYS (KeyMode): kKeysBoth when every system of the launch has the seed whose
-// Philox round keys are in `keys` (a kernel parameter); kKeysHigh when they
-// share its upper 32 bits, so that only the first key word is read from the
-// tile's SysDev and advanced round by round; kKeysNone: both are.
-template <int KEYS>
-__device__ __forceinline__ uint4 philox_block(uint4 ctr, uint32_t k0, uint32_t k1, const PhiloxKeys& keys) {
-    if (KEYS == kKeysBoth) return philox4x32_10(ctr, keys);
-    if (KEYS == kKeysHigh) return philox4x32_10(ctr, k0, keys);
-    return philox4x32_10(ctr, k0, k1);
-}
-
 // Register cap per instance.  80 (six 128-thread CTAs, 24 warps per SM) is
 // what the general instances need without spilling; the instances that read
 // their Philox round keys from the parameter bank fit in 72 without spilling,
@@ -1297,9 +1300,12 @@ int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_c
 
 // Opt the sweep kernels in to the largest dynamic shared memory once, outside
 // any stream capture (called when a system is created).
-template <int MODE, bool LINEAR>
+template <int MODE, int KEYS>
 static cudaError_t allow_smem(int bytes) {
-    return cudaFuncSetAttribute(k_sweep<MODE, LINEAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_sweep<MODE, false, KEYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep_linear<MODE, KEYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
 }
 
 int configure_kernels() {
@@ -1319,15 +1325,20 @@ int configure_kernels() {
     cudaError_t ef = cudaMemcpyToSymbol(c_fold, fold_tab, sizeof fold_tab);
     if (ef != cudaSuccess) return (int)ef;
     const int bytes = (int)sweep_smem_bytes(kMaxTileBeads, kMaxLength);
-    cudaError_t e = allow_smem<kMoveOnly, false>(bytes);
-    if (e == cudaSuccess) e = allow_smem<kMoveGrid, false>(bytes);
-    if (e == cudaSuccess) e = allow_smem<kGridOnly, false>(bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sweep_linear<kMoveOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sweep_linear<kMoveGrid>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sweep_linear<kGridOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaSuccess;
+    for (int keys = kKeysNone; keys <= kKeysBoth && e == cudaSuccess; ++keys) {
+        if (keys == kKeysNone) {
+            e = allow_smem<kGridOnly, kKeysNone>(bytes);
+            if (e == cudaSuccess) e = allow_smem<kMoveOnly, kKeysNone>(bytes);
+            if (e == cudaSuccess) e = allow_smem<kMoveGrid, kKeysNone>(bytes);
+        } else if (keys == kKeysHigh) {
+            e = allow_smem<kMoveOnly, kKeysHigh>(bytes);
+            if (e == cudaSuccess) e = allow_smem<kMoveGrid, kKeysHigh>(bytes);
+        } else {
+            e = allow_smem<kMoveOnly, kKeysBoth>(bytes);
+            if (e == cudaSuccess) e = allow_smem<kMoveGrid, kKeysBoth>(bytes);
+        }
+    }
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return (int)e;
 }
@@ -1359,6 +1370,7 @@ static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, L
                           cudaStream_t st) {
     if (mtb > kMaxTileBeads || ml > kMaxLength || sh.threads > 256 || sh.threads < 32) return (int)cudaErrorInvalidValue;
     const int blocks = sh.blocks > 0 ? sh.blocks : n_tiles;
+    const int keys = MODE == kGridOnly ? kKeysNone : sh.keyed;
     if (sh.linear && ml <= 64) {
         // tiles whose chains fill warps exactly run the barrier-free kernel,
         // the others (sh.flat_list) the block-wide one: one launch each
@@ -1377,10 +1389,20 @@ static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, L
         const int wb = ((sh.max_chains + nw - 1) / nw) * ml;
         const size_t smem = (size_t)nw * (3 * wb + (wb + 1) / 2) * sizeof(float);
         if (smem > sweep_smem_bytes(kMaxTileBeads, kMaxLength)) return (int)cudaErrorInvalidValue;
-        k_sweep_linear<MODE><<<blocks, sh.threads, smem, st>>>(tiles, nullptr, n_tiles, wb, acc);
+        if (keys == kKeysBoth)
+            k_sweep_linear<MODE, kKeysBoth><<<blocks, sh.threads, smem, st>>>(tiles, nullptr, n_tiles, wb, acc, sh.keys);
+        else if (keys == kKeysHigh)
+            k_sweep_linear<MODE, kKeysHigh><<<blocks, sh.threads, smem, st>>>(tiles, nullptr, n_tiles, wb, acc, sh.keys);
+        else
+            k_sweep_linear<MODE, kKeysNone><<<blocks, sh.threads, smem, st>>>(tiles, nullptr, n_tiles, wb, acc, sh.keys);
     } else {
         const size_t smem = sweep_smem_bytes(mtb, ml);
-        k_sweep<MODE, false><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml, acc);
+        if (keys == kKeysBoth)
+            k_sweep<MODE, false, kKeysBoth><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml, acc, sh.keys);
+        else if (keys == kKeysHigh)
+            k_sweep<MODE, false, kKeysHigh><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml, acc, sh.keys);
+        else
+            k_sweep<MODE, false, kKeysNone><<<blocks, sh.threads, smem, st>>>(tiles, n_tiles, mtb, ml, acc, sh.keys);
     }
     return (int)cudaGetLastError();
 }

@@ -210,13 +210,33 @@ def test_batch_bit_identical_to_alone(nb):
         s.close()
 
 
+def _comb_spec(nb, seed):
+    from new_arch_b200.spec import Arch, SystemSpec, interaction_matrix
+    backbone = 9
+    mono = [0] * backbone
+    bonds = [[i, i + 1] for i in range(backbone - 1)]
+    for j in range(0, backbone, 3):       # two-bead side chains at every third backbone bead
+        a = len(mono)
+        mono += [1, 1]
+        bonds += [[j, a], [a, a + 1]]
+    return SystemSpec(2, 6, 6, 5, 6.0, 6.0, 5.0, interaction_matrix(2, 15.0, 50.0), len(mono), 3.0 / (2 * 0.49), 0.5,
+                      seed, nb.HAM_SCMF0, nb.FIELD_EVERY, 32, [Arch(len(mono), 60, mono, bonds, 0.7 / np.sqrt(3.0))])
+
+
+@pytest.mark.parametrize("kernel", ["register", "long_chains", "any_graph"])
 @pytest.mark.parametrize("seeds", ["one", "same_high_word", "distinct_high_words"])
-def test_batch_key_modes_match_oracle(nb, seeds):
+def test_batch_key_modes_match_oracle(nb, seeds, kernel):
     """Systems batched into one launch take their Philox round keys from the
     kernel parameters when they share a seed, the second key word's only when
     they share the seed's upper 32 bits, and neither otherwise (each tile's
-    key advanced in registers).  All three launch kinds equal the oracle."""
-    specs = nb.spec.batched_mix(4, mix_seed=11, edge_scale=0.25)
+    key advanced in registers).  All three launch kinds equal the oracle, for
+    each move kernel: a batch with a chain longer than 64 beads runs the
+    long-chain kernel, one with a branched architecture the general one."""
+    specs = nb.spec.batched_mix(3, mix_seed=11, edge_scale=0.25)
+    if kernel == "long_chains":
+        specs.append(nb.spec.diblock_melt(20, 80, 0.5, (6, 6, 6), 20.0, 50.0))
+    elif kernel == "any_graph":
+        specs.append(_comb_spec(nb, 0))
     for i, sp in enumerate(specs):
         sp.seed = {"one": 77, "same_high_word": 77 + i, "distinct_high_words": 77 + (i << 33)}[seeds]
     systems = [nb.System(sp) for sp in specs]
@@ -227,7 +247,7 @@ def test_batch_key_modes_match_oracle(nb, seeds):
     for i, (sp, s) in enumerate(zip(specs, systems)):
         orc = oracle_for(sp)
         orc.step(4)
-        compare_state(s, orc, f"{seeds} batch member {i}")
+        compare_state(s, orc, f"{kernel} {seeds} batch member {i}")
     b.close()
     for s in systems:
         s.close()
