@@ -1,14 +1,22 @@
 // sm_100a kernels of the SCMF engine.
 //
 //   k_init_coords   random-walk chains (device_function.cu:140-207)
-//   k_sweep<mode>   one MC sweep over tiles of whole chains, staged in shared
-//                   memory: odd/even (graph-colour) half-sweeps of smart-MC
-//                   trials (device_function.cu:444-454, 509-799), then the
-//                   per-type cell counts of the final positions
-//                   (device_function.cu:471-508) and the bond energy
+//   k_sweep_reg     one MC sweep of linear chains of up to 64 beads, positions
+//                   in registers (a thread per bead pair): odd/even half-sweeps
+//                   of smart-MC trials (device_function.cu:444-454, 509-799),
+//                   moving one cell count for each accepted move that leaves
+//                   its cell, so counts stay the grid of the positions
+//                   (device_function.cu:471-508); or, in kGridOnly, a gridding
+//                   pass from scratch
+//   k_sweep_linear  the same for longer linear chains, staged per warp in
+//                   shared memory
+//   k_sweep         the same for any bond graph (graph-colour half-sweeps)
 //   k_field<fused>  counts -> omega (SCMF0, device_function.cu:373-412) with the
-//                   field-energy reduction; in the fused step it also clears the
-//                   other counts buffer and closes the sweep (step, statistics)
+//                   field-energy reduction; in the fused step the block that
+//                   finishes a system's last tile closes the sweep (step,
+//                   statistics, averaging sample)
+//   k_close, k_bond_energy, k_observables, k_validate_*, transposes: the
+//                   reductions and checks around the step
 //
 // Built with --fmad=false -prec-div=true -prec-sqrt=true: positions and counts
 // are bit-identical to the CPU oracle, whatever the tiling or launch shape.
