@@ -6,8 +6,8 @@
 //                                      device_function.cu:313-360).  Beads of a
 //                                      chain are contiguous; chains are grouped
 //                                      by architecture (init_config.cu:610-629).
-//   chain_id     uint32[n_chains]     storage slot -> global chain id (the RNG
-//                                      key), so chains can be reordered in space
+//   chain_id     uint32[n_chains]     storage slot -> global chain id (the first
+//                                      Philox counter word), so chains can be reordered in space
 //                                      without changing any result.
 //   counts[2]    uint32[n_types*n_cells] (or uint16 pairs)  per-type cell counts,
 //                                      [type][z][y][x].  counts[cur] is kept the
