@@ -198,10 +198,14 @@ scmf_status scmf_debug_math(uint32_t key_lo, uint32_t key_hi, int32_t n, uint32_
  * energy partials, is a fixed array in the library's device memory: at most
  * 8,388,608 cells (2048 tiles of 4096); larger grids are rejected with
  * SCMF_E_INVALID.  Every GPU that loads the library holds that 16 KiB until
- * the process exits.  The first call on a device looks the array's address up
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
- * All calls share the array and each overwrites it: calls that overlap on the
- * GPU (different streams, or devices sharing one context) race. */
+ * the process exits.  The first call in a device's context looks the array's
+ * address up (cudaGetSymbolAddress) and keeps it with that context's id; the
+ * first call after the context was re-created (cudaDeviceReset, or a primary
+ * context released and retained again) looks it up anew.  Make those first
+ * calls before any stream capture.  There is one array per device, shared by
+ * every call on that device, and each call overwrites it: calls on the same
+ * device that overlap on the GPU (from any stream or any host thread) race;
+ * calls on different devices do not. */
 scmf_status scmf_update_omega_noalloc(const uint32_t* d_counts, float* d_omega, int32_t n_types, int64_t n_cells,
                                       double field_scaling, const double* xn, int32_t reference_nbeads,
                                       int32_t hamiltonian, double* d_energy, void* stream);

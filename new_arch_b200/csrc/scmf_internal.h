@@ -123,7 +123,7 @@ enum SweepMode : int { kMoveOnly = 0, kMoveGrid = 1, kGridOnly = 2 };
 
 // What k_close does for each system of a launch.
 enum CloseMode : int {
-    kCloseMove = 1, kCloseField = 2, kCloseBond = 4, kCloseFlip = 8, kCloseAdvance = 16,
+    kCloseMove = 1, kCloseField = 2, kCloseBond = 4, kCloseAdvance = 16,
     kCloseAverage = 32,  // count a time-averaged density sample when the sweep took one
     kSweepClose = kCloseMove | kCloseField | kCloseAdvance | kCloseAverage
 };

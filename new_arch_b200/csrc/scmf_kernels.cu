@@ -20,6 +20,7 @@
 //
 // Built with --fmad=false -prec-div=true -prec-sqrt=true: positions and counts
 // are bit-identical to the CPU oracle, whatever the tiling or launch shape.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -961,7 +962,6 @@ __device__ void close_system(SysDev* S, const double* part, int count, int mode,
         }
         if ((mode & kCloseAverage) && S->avg && S->avg_every && ((S->step + 1u) % S->avg_every) == 0u)
             S->avg_samples += 1ull;
-        if (mode & kCloseFlip) S->cur ^= 1u;
         if (mode & kCloseAdvance) S->step += 1u;
     }
     __syncthreads();
@@ -1573,25 +1573,60 @@ __global__ void __launch_bounds__(256) k_sum_partials(const double* __restrict__
     if (threadIdx.x == 0) *out = s[0];
 }
 
-// Device address of the scratch array, looked up once per device (with that
-// device current) and cached.  The host-side name of a __device__ variable is
-// only a stand-in for it and must never be passed to a kernel.
+// The id of the calling thread's current CUDA context (0 when none is current
+// or the driver cannot tell).  Taken through the driver entry points, so the
+// library needs no link against libcuda.
+static unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, nullptr) == cudaSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, nullptr) == cudaSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of the scratch array for the current device.  The host-side
+// name of a __device__ variable is only a stand-in for it and must never be
+// passed to a kernel.  The address is looked up (with the device current) on
+// the first call in a context and cached with that context's id; a context
+// created later on the device (after cudaDeviceReset, or when the primary
+// context was released and retained again) loads the module anew, so its id
+// differs and the address is looked up again.  Without a context id from the
+// driver it is looked up on every call.
 static double* noalloc_scratch(int device, cudaError_t* err) {
+    struct Entry {
+        unsigned long long ctx;
+        double* addr;
+    };
     static std::mutex mu;
-    static double* addr[64] = {nullptr};
+    static Entry cache[64] = {};
     if (device < 0 || device >= 64) {
         *err = cudaErrorInvalidDevice;
         return nullptr;
     }
     std::lock_guard<std::mutex> g(mu);
-    if (!addr[device]) {
-        void* p = nullptr;
-        *err = cudaGetSymbolAddress(&p, g_noalloc_partials);
-        if (*err != cudaSuccess) return nullptr;
-        addr[device] = static_cast<double*>(p);
+    const unsigned long long ctx = current_context_id();
+    if (ctx != 0 && cache[device].ctx == ctx && cache[device].addr) {
+        *err = cudaSuccess;
+        return cache[device].addr;
     }
-    *err = cudaSuccess;
-    return addr[device];
+    void* p = nullptr;
+    *err = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (*err != cudaSuccess) return nullptr;
+    // the lookup makes the device's context current if none was: take its id now
+    cache[device] = Entry{current_context_id(), static_cast<double*>(p)};
+    return cache[device].addr;
 }
 
 }  // namespace scmf

@@ -25,6 +25,18 @@ def _cpu_has_fma() -> bool:
         return False
 
 
+def reference_dir() -> str | None:
+    """The reference checkout the recipes in this folder read (the Makefile's
+    REF, which the environment variable REF overrides), or None when it is not
+    present on this machine."""
+    try:
+        r = subprocess.run(["make", "-s", "-C", _HERE, "print-ref"], check=True, capture_output=True, text=True)
+    except (OSError, subprocess.CalledProcessError):
+        return None
+    path = r.stdout.strip()
+    return path if path and os.path.isdir(path) else None
+
+
 def build(ref: bool = False) -> None:
     """Compile the oracle (and the reference's vtk.c into _ref/ when asked)."""
     targets = ["all"] + (["ref"] if ref else [])

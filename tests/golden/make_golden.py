@@ -3,7 +3,9 @@
 Run here (where the reference is mounted) after `make -C oracle ref`, which
 compiles the reference's own vtk.c into oracle/_ref/vtk:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py [reference checkout]
+
+without an argument it reads the checkout the oracle's Makefile names (REF).
 
 Outputs (all small, committed):
   configuration.dat, polymer.dat     the reference's input files (2 types)
@@ -94,4 +96,12 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    else:
+        sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+        from oracle.oracle import reference_dir
+        ref = reference_dir()
+        if ref is None:
+            sys.exit("reference checkout not found (set REF)")
+        main(ref)

@@ -18,7 +18,9 @@ from new_arch_b200.spec import SystemSpec
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REF = "/root/reference"
+from oracle.oracle import reference_dir
+
+REF = reference_dir() or ""
 HAS_GPU = False
 try:
     import torch
