@@ -43,9 +43,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--forms", choices=["all", "plain", "batched", "served"], default="all")
+    ap.add_argument("--forms", choices=["all", "plain", "blend", "batched", "served"], default="all")
     ap.add_argument("--batched-sweeps", type=int, default=100)
-    ap.add_argument("--served-requests", type=int, default=2000)
+    ap.add_argument("--served-requests", type=int, default=20000)
+    ap.add_argument("--capacity-requests", type=int, default=3000)
     ap.add_argument("--served-rate", type=float, default=200.0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -181,7 +182,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "parallelism": "host threads", "l2": "inputs larger than L2"},
+            "config": {"workload": WORKLOAD, "beads": spec.n_beads, "cells": spec.n_cells,
+                       "parallelism": "host threads", "l2": "inputs larger than L2"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -275,11 +277,15 @@ def run_ours(args):
             "phases": {"move_grid_ms": ms_move / args.steps, "field_ms": ms_field / args.steps,
                        "field_gbs": field_gbs, "field_frac": field_gbs / peak}}
 
-    # ---- batched vs plain on the same 256-system mix, and the served stream (rank-local)
+    # ---- the blend (largest single-GPU configuration), batched vs plain on the
+    # same 256-system mix, and the served stream (rank-local)
+    if args.forms in ("all", "blend"):
+        line["configs"] = {"blend": run_blend(nb, args, peak)}
     if args.forms in ("all", "batched"):
-        line["batched"] = run_batched(nb, batched_mix, args, torch)
+        line["batched"] = run_batched(nb, batched_mix, args, torch, peak)
     if args.forms in ("all", "served"):
         line["served"] = run_served(nb, served_request, args)
+        line["served_capacity"] = run_capacity(nb, served_request, args)
 
     # ---- CPU oracle on this host (rank 0, N=1 only)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -295,7 +301,31 @@ def run_ours(args):
     return 0
 
 
-def run_batched(nb, batched_mix, args, torch):
+def run_blend(nb, args, peak):
+    """The homopolymer blend with a diblock compatibiliser (2M chains: A and B
+    homopolymers of N=64 and 10 % AB diblocks of N=32, 121.6M beads,
+    256x256x64 cells, chiN=15 at N_ref=64, kappaN=40, seed 11): device-timed
+    sweeps with the per-phase HBM fractions."""
+    from new_arch_b200.spec import blend_system
+    spec = blend_system(seed=11)
+    K = args.steps
+    with nb.System(spec) as s:
+        s.init_coords()
+        s.step(args.warmup)
+        ms_move, ms_field, ms_total = s.step_profiled(K)
+        st = s.stats()
+    move_gbs = 24 * spec.n_beads / (ms_move / K / 1e3) / 1e9
+    field_gbs = 8 * spec.n_types * spec.n_cells / (ms_field / K / 1e3) / 1e9
+    return {"workload": "blend: 50% A-homopolymer N=64, 40% B-homopolymer N=64, 10% AB diblock N=32; 2M chains "
+                        "(121.6M beads), 256x256x64 cells, chiN=15 (N_ref=64), kappaN=40, seed 11",
+            "beads": spec.n_beads, "cells": spec.n_cells, "sweeps_timed": K,
+            "bead_moves_per_s": spec.n_beads * K / (ms_total / 1e3), "ms_per_step": ms_total / K,
+            "move_ms": ms_move / K, "field_ms": ms_field / K,
+            "move_gbs": move_gbs, "move_frac": move_gbs / peak, "field_gbs": field_gbs, "field_frac": field_gbs / peak,
+            "accept_ratio": st["last_accepts"] / spec.n_beads}
+
+
+def run_batched(nb, batched_mix, args, torch, peak):
     specs = batched_mix(256)
     st = torch.cuda.Stream()
     systems = [nb.System(sp, stream=st.cuda_stream) for sp in specs]
@@ -323,6 +353,9 @@ def run_batched(nb, batched_mix, args, torch):
     e1.record(st)
     e1.synchronize()
     batched_ms = e0.elapsed_time(e1)
+    # per-phase device time of the batched sweeps (launch by launch, no graph)
+    pm, pf, _ = b.step_profiled(10)
+    cells_all = sum(sp.n_cells * sp.n_types for sp in specs)
     b.close()
     for x in systems:
         x.close()
@@ -338,7 +371,10 @@ def run_batched(nb, batched_mix, args, torch):
     return {"workload": "256 diblock systems, edges {16..64}^3, N {16..64}, 100 sweeps each", "beads": beads,
             "sweeps": K, "plain_bead_moves_per_s": plain, "batched_bead_moves_per_s": batched,
             "batched_over_plain": batched / plain, "tune": tune, "gpu_launches_batched": per_batch * K,
-            "gpu_launches_plain": per_sys * K}
+            "gpu_launches_plain": per_sys * K,
+            "move_frac": 24 * beads / (pm / 10 / 1e3) / 1e9 / peak,
+            "field_frac": 8 * cells_all / (pf / 10 / 1e3) / 1e9 / peak,
+            "phase_ms": {"move": pm / 10, "field": pf / 10}}
 
 
 def run_served(nb, served_request, args):
@@ -368,6 +404,31 @@ def run_served(nb, served_request, args):
             "requests": n, "ok": ok, "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)), "bead_moves_per_s": moves / span,
             "offered_bead_moves_per_s": moves / float(arrive[-1]), "wall_s": wall}
+
+
+def run_capacity(nb, served_request, args):
+    """Capacity of the served form: requests drawn as in the served stream, all
+    submitted at once (an offered rate far above what the GPU sustains), so
+    the bead-moves/s over the makespan is the largest the server sustains."""
+    from new_arch_b200.server import Server
+    rng = np.random.default_rng(777)
+    n = args.capacity_requests
+    reqs = [served_request(rng, seed=80_000 + i) for i in range(n)]
+    done = []
+    with Server(150 * 10**9) as srv:
+        t0 = time.perf_counter()
+        for sp, k in reqs:
+            srv.submit(sp, k, want_counts=False)
+        while len(done) < n:
+            done += srv.poll(256, 200)
+        wall = time.perf_counter() - t0
+    lat = np.array([r["t_done"] - r["t_submit"] for r in done])
+    moves = sum(r["n_beads"] * r["n_sweeps"] for r in done)
+    span = max(r["t_done"] for r in done) - min(r["t_submit"] for r in done)
+    return {"workload": f"{n} requests as in the served stream, all submitted at t=0", "requests": n,
+            "ok": sum(1 for r in done if r["status"] == 0), "bead_moves_per_s": moves / span, "makespan_s": span,
+            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+            "wall_s": wall}
 
 
 def main():

@@ -347,6 +347,11 @@ scmf_status scmf_batch_create(scmf_system* const* systems, int32_t n, const scmf
 scmf_status scmf_batch_step(scmf_batch* b, int32_t n_sweeps);
 /* The same, enqueued on the batch's stream without waiting. */
 scmf_status scmf_batch_step_async(scmf_batch* b, int32_t n_sweeps);
+/* scmf_step_profiled for a batch: its sweeps launch by launch with CUDA events
+ * on the batch's stream; the move time covers both move launches of a plan
+ * that runs them side by side.  Same results as scmf_batch_step. */
+scmf_status scmf_batch_step_profiled(scmf_batch* b, int32_t n_sweeps, float* ms_move, float* ms_field,
+                                     float* ms_total);
 /* Times candidate tunings on snapshots of the batch's systems (their state is
  * restored afterwards) and installs the fastest; *out receives it. */
 scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps_per_trial, scmf_tune* out);

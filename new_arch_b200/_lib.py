@@ -147,6 +147,7 @@ SIGNATURES = {
     "scmf_batch_create": (_i32, [_pvp, _i32, C.POINTER(Tune), _vp, _pvp]),
     "scmf_batch_step": (_i32, [_vp, _i32]),
     "scmf_batch_step_async": (_i32, [_vp, _i32]),
+    "scmf_batch_step_profiled": (_i32, [_vp, _i32, _pf32, _pf32, _pf32]),
     "scmf_batch_autotune": (_i32, [_vp, _i32, C.POINTER(Tune)]),
     "scmf_batch_get_tune": (_i32, [_vp, C.POINTER(Tune)]),
     "scmf_batch_destroy": (None, [_vp]),

@@ -437,9 +437,12 @@ scmf_status scmf_step(scmf_system* s, int32_t n) {
     return check_error_word(s);
 }
 
-scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float* ms_field, float* ms_total) {
-    if (!s || n < 0 || !ms_move || !ms_field || !ms_total) return fail(SCMF_E_INVALID, "bad argument");
-    RET(fresh_counts(s));
+// n fused sweeps of a plan enqueued launch by launch, each bracketed by CUDA
+// events on `st`: the summed device time of the move launches (both tile kinds
+// when the plan forks them), of the field launches, and from the first launch
+// to the end of the last.
+static scmf_status profile_sweeps(const DevPlan& p, cudaStream_t st, int32_t n, float* ms_move, float* ms_field,
+                                  float* ms_total) {
     *ms_move = 0.0f;
     *ms_field = 0.0f;
     *ms_total = 0.0f;
@@ -448,18 +451,14 @@ scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float*
     scmf_status rc = SCMF_OK;
     for (auto& e : ev)
         if (cudaEventCreate(&e) != cudaSuccess) rc = fail(SCMF_E_CUDA, "cudaEventCreate failed");
-    const DevPlan& p = s->plan;
-    const LaunchShape ms = p.move_shape();
-    const LaunchShape fs = p.field_shape();
     for (int i = 0; i < n && !rc; ++i) {
-        cudaEventRecord(ev[3 * i], s->stream);
-        int e = launch_sweep(kMoveGrid, p.d_move, p.n_move, p.max_tile_beads, p.max_length, ms, p.d_acc, s->stream);
-        cudaEventRecord(ev[3 * i + 1], s->stream);
-        if (!e) e = launch_field(true, 0, p.d_field, p.n_field, fs, p.d_ef, kSweepClose, s->stream);
-        cudaEventRecord(ev[3 * i + 2], s->stream);
-        if (e) rc = fail(SCMF_E_CUDA, "launch: %s", cudaGetErrorString((cudaError_t)e));
+        cudaEventRecord(ev[3 * i], st);
+        rc = p.enqueue_move(st);
+        cudaEventRecord(ev[3 * i + 1], st);
+        if (!rc) rc = p.enqueue_field(st);
+        cudaEventRecord(ev[3 * i + 2], st);
     }
-    if (!rc && cudaStreamSynchronize(s->stream) != cudaSuccess) rc = fail(SCMF_E_CUDA, "sweep failed");
+    if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = fail(SCMF_E_CUDA, "sweep failed");
     for (int i = 0; i < n && !rc; ++i) {
         float a = 0, b = 0;
         cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]);
@@ -470,7 +469,13 @@ scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float*
     if (!rc) cudaEventElapsedTime(ms_total, ev[0], ev[3 * (size_t)n - 1]);
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
-    if (rc) return rc;
+    return rc;
+}
+
+scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float* ms_field, float* ms_total) {
+    if (!s || n < 0 || !ms_move || !ms_field || !ms_total) return fail(SCMF_E_INVALID, "bad argument");
+    RET(fresh_counts(s));
+    RET(profile_sweeps(s->plan, s->stream, n, ms_move, ms_field, ms_total));
     return check_error_word(s);
 }
 
@@ -662,6 +667,17 @@ scmf_status scmf_batch_step_async(scmf_batch* b, int32_t n) {
 scmf_status scmf_batch_step(scmf_batch* b, int32_t n) {
     RET(scmf_batch_step_async(b, n));
     CK(cudaStreamSynchronize(b->stream));
+    return SCMF_OK;
+}
+
+scmf_status scmf_batch_step_profiled(scmf_batch* b, int32_t n, float* ms_move, float* ms_field, float* ms_total) {
+    if (!b || n < 0 || !ms_move || !ms_field || !ms_total) return fail(SCMF_E_INVALID, "bad argument");
+    for (auto* s : b->systems) {
+        RET(fresh_counts(s));
+        if (s->stream != b->stream) CK(cudaStreamSynchronize(s->stream));
+    }
+    RET(profile_sweeps(b->plan, b->stream, n, ms_move, ms_field, ms_total));
+    for (auto* s : b->systems) RET(check_error_word(s));
     return SCMF_OK;
 }
 

@@ -398,6 +398,11 @@ scmf_status DevPlan::enqueue_close(int mode, cudaStream_t st) const {
 }
 
 scmf_status DevPlan::enqueue_sweep(cudaStream_t st) const {
+    const scmf_status rc = enqueue_move(st);
+    return rc ? rc : enqueue_field(st);
+}
+
+scmf_status DevPlan::enqueue_move(cudaStream_t st) const {
     if (side && n_warp > 0 && n_flat > 0) {
         LaunchShape warp = move_shape(), flat = move_shape();
         warp.part = 1;
@@ -411,6 +416,10 @@ scmf_status DevPlan::enqueue_sweep(cudaStream_t st) const {
     } else {
         CKL(launch_sweep(kMoveGrid, d_move, n_move, max_tile_beads, max_length, move_shape(), d_acc, st));
     }
+    return SCMF_OK;
+}
+
+scmf_status DevPlan::enqueue_field(cudaStream_t st) const {
     CKL(launch_field(true, 0, d_field, n_field, field_shape(), d_ef, kSweepClose, st));
     return SCMF_OK;
 }

@@ -109,8 +109,12 @@ struct DevPlan {
     LaunchShape move_shape() const;
     LaunchShape field_shape() const;
     int warps_per_tile() const { return tune.threads_move / 32; }
-    // one fused sweep (move+grid, field, close) enqueued on `st`
+    // one fused sweep (move+grid, field, close) enqueued on `st`: the move
+    // launches (two side by side when the plan has both tile kinds), then the
+    // field launch whose last tile per system closes the sweep
     scmf_status enqueue_sweep(cudaStream_t st) const;
+    scmf_status enqueue_move(cudaStream_t st) const;
+    scmf_status enqueue_field(cudaStream_t st) const;
     scmf_status enqueue_close(int mode, cudaStream_t st) const;
     scmf_status run_sweeps(cudaStream_t st, int n);
 };

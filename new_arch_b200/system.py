@@ -243,6 +243,14 @@ class Batch:
     def step_async(self, n_sweeps: int = 1) -> None:
         check(lib().scmf_batch_step_async(self._h, int(n_sweeps)))
 
+    def step_profiled(self, n_sweeps: int = 1):
+        """Runs n sweeps launch by launch with CUDA events; returns the summed
+        device milliseconds of the move launches, of the field launches, and
+        the device time from the first launch to the end of the last."""
+        a, b, t = C.c_float(), C.c_float(), C.c_float()
+        check(lib().scmf_batch_step_profiled(self._h, int(n_sweeps), C.byref(a), C.byref(b), C.byref(t)))
+        return a.value, b.value, t.value
+
     def autotune(self, sweeps_per_trial: int = 2) -> dict:
         t = _lib.Tune()
         check(lib().scmf_batch_autotune(self._h, int(sweeps_per_trial), C.byref(t)))

@@ -95,6 +95,8 @@ def lib():
     L.orc_normals3.argtypes = [u32p, f32p, f32p, f32p]
     L.orc_u01.restype = C.c_float
     L.orc_u01.argtypes = [C.c_uint32]
+    L.orc_trial_energy.restype = C.c_float
+    L.orc_trial_energy.argtypes = [vp, i32, i32, f32p, f32p, f32p, C.c_float, C.c_float, C.c_float, f32p]
     L.orc_fold.restype = i32
     L.orc_fold.argtypes = [C.c_float, C.c_float, i32]
     _lib = L
@@ -229,6 +231,15 @@ class OracleSystem:
         out = np.zeros(self.n_types * self.n_cells, dtype=np.uint64)
         n = lib().orc_average_get(self._h, _p(out, C.c_uint64))
         return out, int(n)
+
+    def trial_energy(self, arch, b, xyz, n):
+        """(energy change, proposed position) of one trial of bead b of a chain of
+        architecture `arch` at positions xyz[L, 3] with the normals n[3]."""
+        a = np.ascontiguousarray(np.asarray(xyz, dtype=np.float32).T)
+        p = np.zeros(3, dtype=np.float32)
+        e = lib().orc_trial_energy(self._h, int(arch), int(b), _p(a[0], C.c_float), _p(a[1], C.c_float),
+                                   _p(a[2], C.c_float), float(n[0]), float(n[1]), float(n[2]), _p(p, C.c_float))
+        return e, p
 
     def set_fault(self, no_smc: bool):
         """Plant a known mistake (drop the smart-MC correction) to test the tests."""

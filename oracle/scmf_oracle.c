@@ -463,13 +463,13 @@ float orc_dE_closed(int deg, const float* q, const float* p, const float* d, flo
     return dE_closed(c, (A * c) * 0.25f, fx, fy, fz, d[0], d[1], d[2]);
 }
 
-/* One smart-MC trial of bead b (device_function.cu:637-717, 562-588, 444-454)
- * with the Gaussian triple (n0, n1, n2) and the Metropolis word aw: force from
- * the bonded neighbours (ascending order), displacement d = A f + R xi, energy
- * change omega[new cell] - omega[old cell] + the closed form above, Metropolis
- * test.  Returns 1 if accepted. */
-static inline int move_bead(const orc_system* s, const orc_arch* a, int b, float* X, float* Y, float* Z,
-                            float n0, float n1, float n2, uint32_t aw) {
+/* The energy change of one smart-MC trial of bead b (device_function.cu:637-717,
+ * 562-588) with the Gaussian triple (n0, n1, n2): force from the bonded
+ * neighbours (ascending order), displacement d = A f + R xi, proposed position
+ * (*px, *py, *pz), and omega[new cell] - omega[old cell] + the closed form
+ * above. */
+static inline float trial_energy(const orc_system* s, const orc_arch* a, int b, const float* X, const float* Y,
+                                 const float* Z, float n0, float n1, float n2, float* px, float* py, float* pz) {
     const int* nb = a->nbr + b * ORC_MAX_DEG;
     const int deg = a->deg[b];
     const float k2 = s->k2, A = s->A, R = s->R;
@@ -484,12 +484,14 @@ static inline int move_bead(const orc_system* s, const orc_arch* a, int b, float
     const float dx = fmaf(A, fx, R * n0);
     const float dy = fmaf(A, fy, R * n1);
     const float dz = fmaf(A, fz, R * n2);
-    const float px = x + dx, py = y + dy, pz = z + dz;
+    *px = x + dx;
+    *py = y + dy;
+    *pz = z + dz;
     const float c = s->cdeg[deg], ac4 = s->ac4deg[deg];
     const int t = a->type[b];
     const float* W = s->omega + (int64_t)t * s->n_cells;
     const float w_old = W[cell_of(s, x, y, z)];
-    const float w_new = W[cell_of(s, px, py, pz)];
+    const float w_new = W[cell_of(s, *px, *py, *pz)];
     float eb;
     if (s->fault_no_smc) {  /* the bond energy change alone, (c/2)|d|^2 - f.d, without the smart-MC correction */
         const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -498,7 +500,16 @@ static inline int move_bead(const orc_system* s, const orc_arch* a, int b, float
     } else {
         eb = dE_closed(c, ac4, fx, fy, fz, dx, dy, dz);
     }
-    const float dE = (w_new - w_old) + eb;
+    return (w_new - w_old) + eb;
+}
+
+/* One smart-MC trial of bead b (device_function.cu:637-717, 562-588, 444-454)
+ * with the Gaussian triple (n0, n1, n2) and the Metropolis word aw.  Returns 1
+ * if accepted (the bead then sits at the proposed position). */
+static inline int move_bead(const orc_system* s, const orc_arch* a, int b, float* X, float* Y, float* Z,
+                            float n0, float n1, float n2, uint32_t aw) {
+    float px, py, pz;
+    const float dE = trial_energy(s, a, b, X, Y, Z, n0, n1, n2, &px, &py, &pz);
     /* Metropolis: accept if dE < 0, else if log(u) < -dE.  log(u) >= -23 ln2
      * > -17 for every u the generator yields, so dE >= 17 always rejects. */
     int acc;
@@ -507,6 +518,15 @@ static inline int move_bead(const orc_system* s, const orc_arch* a, int b, float
     else acc = 0;
     if (acc) { X[b] = px; Y[b] = py; Z[b] = pz; }
     return acc;
+}
+
+/* trial_energy() of bead b of a chain of architecture `arch` whose positions
+ * are the chain-local arrays X, Y, Z; p_out receives the proposed position.
+ * For the checks against the reference's own trial functions. */
+float orc_trial_energy(const orc_system* s, int arch, int b, const float* X, const float* Y, const float* Z, float n0,
+                       float n1, float n2, float* p_out) {
+    const orc_arch* a = &s->arch[arch];
+    return trial_energy(s, a, b, X, Y, Z, n0, n1, n2, p_out, p_out + 1, p_out + 2);
 }
 
 /* One trial of bead b: its Philox block (chain, b, step, 0) gives the

@@ -100,6 +100,11 @@ uint32_t orc_accept_word(const uint32_t w[4]);
 int   orc_fold(float x, float inv_d, int n);
 double orc_dE_literal(int deg, const float* q, const float* p, const float* d, double k, double A);
 float  orc_dE_closed(int deg, const float* q, const float* p, const float* d, float k2, float A);
+/* energy change of one trial of bead b of a chain of architecture `arch`
+ * (chain-local positions X, Y, Z) with the normals n0..n2; p_out[3] gets the
+ * proposed position */
+float  orc_trial_energy(const orc_system* s, int arch, int b, const float* X, const float* Y, const float* Z, float n0,
+                        float n1, float n2, float* p_out);
 
 #ifdef __cplusplus
 }
