@@ -247,17 +247,24 @@ def run_ours(args):
     pinned = torch.empty(xyz.size, dtype=torch.float32, pin_memory=True)
     pinned.numpy()[:] = xyz.reshape(-1)
     host_in = pinned.numpy()
+    import ctypes
+    stat_bytes = ctypes.sizeof(nb._lib.Stats)
+    stats_host = torch.empty(stat_bytes * args.steps, dtype=torch.uint8, pin_memory=True)
     barrier()
     t0 = time.perf_counter()
     s.set_coords(host_in)
-    for _ in range(args.steps):
-        s.step_stats(1)
+    for k in range(args.steps):
+        s.step_stats_async(1, stats_host.data_ptr() + k * stat_bytes)
+    s.synchronize()
     cnt = s.counts()
     e2e_s = allmax(time.perf_counter() - t0)
+    last = nb.System.stats_at(stats_host.data_ptr() + (args.steps - 1) * stat_bytes)
+    assert last["step"] == st["step"] + args.steps and last["error_word"] == 0, last
     e2e = {"value": whole_job_rate(beads_all, args.steps, e2e_s), "unit": UNIT,
            "h2d_bytes_per_step": xyz.nbytes / args.steps,
-           "d2h_bytes_per_step": (64 * args.steps + cnt.nbytes) / args.steps,
-           "how": "wall clock around scmf_set_coords(pinned host xyz) + K x scmf_step_stats(1) + scmf_get_counts"}
+           "d2h_bytes_per_step": (stat_bytes * args.steps + cnt.nbytes) / args.steps,
+           "how": "wall clock around scmf_set_coords(pinned host xyz) + K x scmf_step_stats_async(1) (each sweep's "
+                  "statistics copied to pinned host memory) + scmf_synchronize + scmf_get_counts"}
     s.close()
     del pinned
 
@@ -346,6 +353,7 @@ def run_batched(nb, batched_mix, args, torch, peak):
     plain_ms = e0.elapsed_time(e1)
     b = nb.Batch(systems, stream=st.cuda_stream)
     tune = b.autotune(2)
+    trials = b.tune_trials()
     b.step_async(1)
     torch.cuda.synchronize()
     e0.record(st)
@@ -374,7 +382,10 @@ def run_batched(nb, batched_mix, args, torch, peak):
             "gpu_launches_plain": per_sys * K,
             "move_frac": 24 * beads / (pm / 10 / 1e3) / 1e9 / peak,
             "field_frac": 8 * cells_all / (pf / 10 / 1e3) / 1e9 / peak,
-            "phase_ms": {"move": pm / 10, "field": pf / 10}}
+            "phase_ms": {"move": pm / 10, "field": pf / 10},
+            "tune_trials": [{"beads_per_tile": t["beads_per_tile"], "threads_move": t["threads_move"],
+                             "persistent_ctas": t["persistent_ctas"], "cells_per_tile": t["cells_per_tile"],
+                             "ms": round(t["ms"], 3)} for t in trials]}
 
 
 def run_served(nb, served_request, args):

@@ -177,6 +177,13 @@ scmf_status scmf_get_sweep_stats(const scmf_system* sys, scmf_stats* out);
  * wait: the loop of a driver that reports every sweep (test.cpp:45-68 prints
  * per check step) costs one host round trip per call instead of three. */
 scmf_status scmf_step_stats(scmf_system* sys, int32_t n_sweeps, scmf_stats* out);
+/* The same without waiting: the sweeps and a copy of their statistics into
+ * *host_out are enqueued on the system's stream, and *host_out is valid after
+ * the next scmf_synchronize (or any other wait on that stream).  host_out
+ * should be page-locked host memory (cudaHostAlloc / cudaHostRegister) for the
+ * copy to run asynchronously, and must stay valid until then.  e_bond is NaN,
+ * as in scmf_get_sweep_stats. */
+scmf_status scmf_step_stats_async(scmf_system* sys, int32_t n_sweeps, scmf_stats* host_out);
 
 /* Diagnostics: evaluates the device arithmetic (Philox4x32-10 with counter
  * (c0,c1,c2,c3) = (i, 0, 0, 0) and the given key, then log(u01(w.x)),
@@ -355,6 +362,17 @@ scmf_status scmf_batch_step_profiled(scmf_batch* b, int32_t n_sweeps, float* ms_
 /* Times candidate tunings on snapshots of the batch's systems (their state is
  * restored afterwards) and installs the fastest; *out receives it. */
 scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps_per_trial, scmf_tune* out);
+/* One tuning the last scmf_batch_autotune timed, with the device time of its
+ * timed sweeps (milliseconds). */
+typedef struct {
+    scmf_tune tune;
+    float ms;
+    int32_t reserved;
+} scmf_tune_trial;
+/* The trials of the batch's last autotune in the order they ran: *n receives
+ * their number, out[0 .. min(*n, max)) the trials.  No counterpart in the
+ * reference (it has no batched form). */
+scmf_status scmf_batch_tune_trials(const scmf_batch* b, scmf_tune_trial* out, int32_t max, int32_t* n);
 scmf_status scmf_batch_get_tune(const scmf_batch* b, scmf_tune* out);
 void scmf_batch_destroy(scmf_batch* b);
 /* create + step + destroy */

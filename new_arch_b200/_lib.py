@@ -51,6 +51,10 @@ class Tune(C.Structure):
                 ("beads_per_tile", C.c_int32), ("reserved", C.c_int32)]
 
 
+class TuneTrial(C.Structure):
+    _fields_ = [("tune", Tune), ("ms", C.c_float), ("reserved", C.c_int32)]
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_active", C.c_int32), ("sweeps_per_round", C.c_int32),
                 ("use_graph", C.c_int32), ("reserved", C.c_int32)]
@@ -127,6 +131,7 @@ SIGNATURES = {
     "scmf_get_stats": (_i32, [_vp, C.POINTER(Stats)]),
     "scmf_get_sweep_stats": (_i32, [_vp, C.POINTER(Stats)]),
     "scmf_step_stats": (_i32, [_vp, _i32, C.POINTER(Stats)]),
+    "scmf_step_stats_async": (_i32, [_vp, _i32, _vp]),
     "scmf_debug_math": (_i32, [_u32, _u32, _i32, _pu32, _pf32, _pf32, _pf32, _pf32]),
     "scmf_update_omega_noalloc": (_i32, [_vp, _vp, _i32, _i64, _f64, _pf64, _i32, _i32, _vp, _vp]),
     "scmf_write_density": (_i32, [_vp, C.c_char_p, _i64]),
@@ -150,6 +155,7 @@ SIGNATURES = {
     "scmf_batch_step_profiled": (_i32, [_vp, _i32, _pf32, _pf32, _pf32]),
     "scmf_batch_autotune": (_i32, [_vp, _i32, C.POINTER(Tune)]),
     "scmf_batch_get_tune": (_i32, [_vp, C.POINTER(Tune)]),
+    "scmf_batch_tune_trials": (_i32, [_vp, C.POINTER(TuneTrial), _i32, C.POINTER(C.c_int32)]),
     "scmf_batch_destroy": (None, [_vp]),
     "scmf_batch_run": (_i32, [_pvp, _i32, _i32, C.POINTER(Tune)]),
     "scmf_server_create": (_i32, [C.POINTER(ServerOpts), _pvp]),

@@ -584,6 +584,16 @@ scmf_status scmf_step_stats(scmf_system* s, int32_t n, scmf_stats* o) {
     return SCMF_OK;
 }
 
+scmf_status scmf_step_stats_async(scmf_system* s, int32_t n, scmf_stats* host_out) {
+    if (!s || !host_out || n < 0) return fail(SCMF_E_INVALID, "bad argument");
+    RET(fresh_counts(s));
+    RET(s->plan.run_sweeps(s->stream, n));
+    CKL(launch_stats_out(s->d_sys, s->stream));
+    CK(cudaMemcpyAsync(host_out, (const char*)s->d_sys + offsetof(SysDev, stats_out), sizeof(scmf_stats),
+                       cudaMemcpyDeviceToHost, s->stream));
+    return SCMF_OK;
+}
+
 scmf_status scmf_get_stats(const scmf_system* cs, scmf_stats* o) {
     scmf_system* s = const_cast<scmf_system*>(cs);
     if (!s || !o) return fail(SCMF_E_INVALID, "NULL argument");
@@ -678,6 +688,17 @@ scmf_status scmf_batch_step_profiled(scmf_batch* b, int32_t n, float* ms_move, f
     }
     RET(profile_sweeps(b->plan, b->stream, n, ms_move, ms_field, ms_total));
     for (auto* s : b->systems) RET(check_error_word(s));
+    return SCMF_OK;
+}
+
+scmf_status scmf_batch_tune_trials(const scmf_batch* b, scmf_tune_trial* out, int32_t max, int32_t* n) {
+    if (!b || !n || max < 0 || (max > 0 && !out)) return fail(SCMF_E_INVALID, "bad arguments");
+    *n = (int32_t)b->trials.size();
+    for (int32_t i = 0; i < *n && i < max; ++i) {
+        std::memset(&out[i], 0, sizeof out[i]);
+        out[i].tune = b->trials[i].first;
+        out[i].ms = b->trials[i].second;
+    }
     return SCMF_OK;
 }
 
@@ -788,10 +809,11 @@ scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps, scmf_tune* out) {
     };
     scmf_tune best = b->plan.tune;
     float best_ms = 1e30f;
+    b->trials.clear();
     if (!rc) {
         const int tile_beads[] = {1024, 2048, 4096, 8192};
         const int threads[] = {64, 128, 256};
-        const int persist[] = {0, 148 * 4};
+        const int persist[] = {0, sm_count() * 4};
         for (int tb : tile_beads)
             for (int th : threads)
                 for (int pc : persist) {
@@ -803,6 +825,7 @@ scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps, scmf_tune* out) {
                     t.persistent_ctas = pc;
                     float ms = 0;
                     rc = trial(t, &ms);
+                    if (!rc) b->trials.push_back({t, ms});
                     if (!rc && ms < best_ms) {
                         best_ms = ms;
                         best = t;
@@ -816,6 +839,7 @@ scmf_status scmf_batch_autotune(scmf_batch* b, int32_t sweeps, scmf_tune* out) {
             t.cells_per_tile = c;
             float ms = 0;
             rc = trial(t, &ms);
+            if (!rc) b->trials.push_back({t, ms});
             if (!rc && ms < best_ms) {
                 best_ms = ms;
                 best = t;

@@ -464,7 +464,8 @@ using namespace scmf;
 scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
     // systems below ~2.4M beads: four tiles per SM (measured best over the 256-system mix
     // against two and six per SM with 4-warp CTAs)
-    const int64_t target_small = std::max<int64_t>(1, n_beads / (4 * 148));
+    const int sms = sm_count();
+    const int64_t target_small = std::max<int64_t>(1, n_beads / (4 * sms));
     const size_t first_tile = p->move.size();
     const size_t first_field = p->field.size();
     p->fold_kind = std::max(p->fold_kind, fold_kind_of(spec));
@@ -518,7 +519,7 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
     }
     for (size_t i = first_tile; i < p->move.size(); ++i) p->move[i].n_tiles_sys = (int32_t)(p->move.size() - first_tile);
     int64_t cpt_cells = t.cells_per_tile;
-    if (cpt_cells <= 0) cpt_cells = std::min<int64_t>(8192, std::max<int64_t>(1024, n_cells / (4 * 148)));
+    if (cpt_cells <= 0) cpt_cells = std::min<int64_t>(8192, std::max<int64_t>(1024, n_cells / (4 * sms)));
     cpt_cells = (cpt_cells + 3) & ~(int64_t)3;
     const int ntile = (int)((n_cells + cpt_cells - 1) / cpt_cells);
     for (int i = 0; i < ntile; ++i) {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "scmf.h"
@@ -163,6 +164,7 @@ struct scmf_batch {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     scmf::DevPlan plan;
+    std::vector<std::pair<scmf_tune, float>> trials;  // the last autotune's tunings and their times (ms)
 };
 
 namespace scmf {

@@ -96,6 +96,10 @@ struct SysDev {
     // served form gives each request its own sweep count inside a shared
     // round); 0xFFFFFFFF everywhere else
     uint32_t stop_step;
+    uint32_t pad2;
+    // the statistics of the last sweep in the public layout, written by
+    // k_stats_out for asynchronous reads (scmf_step_stats_async)
+    scmf_stats stats_out;
 };
 
 // Work item of the move / grid kernel: a run of whole chains of one architecture.
@@ -191,7 +195,13 @@ struct LaunchShape {
     PhiloxKeys keys;
 };
 
+// Streaming multiprocessors of the current device (read once per device; 148
+// on a B200), for grid and tile sizing.
+int sm_count();
+
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);
+// Writes the statistics of the last sweep into d_sys->stats_out (one thread).
+int launch_stats_out(SysDev* d_sys, void* stream);
 // Move kernels add their accept counts into SysDev::slot_acc (32-way spread);
 // the field kernel writes one energy per tile into ef_part, the bond-energy
 // kernel one per move tile into eb_part; k_close sums and publishes them.

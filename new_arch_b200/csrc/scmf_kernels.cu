@@ -1293,10 +1293,43 @@ int launch_debug_math(uint32_t k0, uint32_t k1, int n, uint32_t* words, float* l
     return (int)cudaGetLastError();
 }
 
+int sm_count() {
+    static std::mutex mu;
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    std::lock_guard<std::mutex> g(mu);
+    if (cached[dev] == 0) {
+        int n = 0;
+        cached[dev] = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0 ? n : 148;
+    }
+    return cached[dev];
+}
+
 static int grid_for(int64_t n, int threads) {
     int64_t b = (n + threads - 1) / threads;
-    if (b > 148 * 32) b = 148 * 32;
+    const int64_t cap = (int64_t)sm_count() * 32;
+    if (b > cap) b = cap;
     return (int)(b < 1 ? 1 : b);
+}
+
+// The statistics of the last sweep in the public layout (scmf_get_sweep_stats).
+__global__ void k_stats_out(SysDev* S) {
+    scmf_stats o;
+    o.step = S->step;
+    o.last_accepts = S->last_accepts;
+    o.total_accepts = S->total_accepts;
+    o.total_moves = S->total_moves;
+    o.e_bond = S->e_bond_step == S->step + 1u ? S->e_bond : __longlong_as_double(0x7FF8000000000000ll);
+    o.e_field = S->e_field;
+    o.error_word = S->error_word;
+    o.reserved = 0u;
+    S->stats_out = o;
+}
+
+int launch_stats_out(SysDev* d_sys, void* stream) {
+    k_stats_out<<<1, 1, 0, (cudaStream_t)stream>>>(d_sys);
+    return (int)cudaGetLastError();
 }
 
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream) {

@@ -126,6 +126,17 @@ class System:
     def step_async(self, n_sweeps: int = 1) -> None:
         check(lib().scmf_step_async(self._h, int(n_sweeps)))
 
+    def step_stats_async(self, n_sweeps: int, host_out_address: int) -> None:
+        """n sweeps and a copy of their statistics into the scmf_stats at
+        host_out_address (page-locked memory), enqueued without waiting; read
+        it with stats_at() after synchronize()."""
+        check(lib().scmf_step_stats_async(self._h, int(n_sweeps), C.c_void_p(host_out_address)))
+
+    @staticmethod
+    def stats_at(address: int) -> dict:
+        st = _lib.Stats.from_address(address)
+        return {k: getattr(st, k) for k, _ in _lib.Stats._fields_ if k != "reserved"}
+
     def step_profiled(self, n_sweeps: int = 1):
         """Runs n sweeps launch by launch with CUDA events; returns the summed
         device milliseconds of the move+grid kernel, of the field kernel, and
@@ -250,6 +261,14 @@ class Batch:
         a, b, t = C.c_float(), C.c_float(), C.c_float()
         check(lib().scmf_batch_step_profiled(self._h, int(n_sweeps), C.byref(a), C.byref(b), C.byref(t)))
         return a.value, b.value, t.value
+
+    def tune_trials(self) -> list:
+        """The tunings the last autotune timed, in order, each with its time (ms)."""
+        n = C.c_int32()
+        check(lib().scmf_batch_tune_trials(self._h, None, 0, C.byref(n)))
+        arr = (_lib.TuneTrial * max(1, n.value))()
+        check(lib().scmf_batch_tune_trials(self._h, arr, n.value, C.byref(n)))
+        return [dict(_tune_dict(arr[i].tune), ms=arr[i].ms) for i in range(n.value)]
 
     def autotune(self, sweeps_per_trial: int = 2) -> dict:
         t = _lib.Tune()
