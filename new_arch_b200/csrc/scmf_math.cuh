@@ -103,9 +103,33 @@ __device__ __forceinline__ float log_floor(float u) {
     return __fmaf_rn(__int2float_rn(e), 0x1.62e430p-1f, -0x1p-10f);
 }
 
+// -2 ln u for u in (0, 1]: the squared Box-Muller radius.  u = 2^k m with m in
+// [sqrt(1/2), sqrt(2)) split off in integers (k from the bits of u minus those
+// of sqrt(1/2)), t = m - 1 exact, -2 log1p(t) = -2t + t^2 Q2(t) with Q2 = -2 Q
+// of log_f (the same fit, scaled by -2 exactly), and -2 k ln2 added with
+// -2 ln2 rounded to FP32 (at most 9e-8 off for the k >= -23 that u01 yields).
+__device__ __forceinline__ float rad2_f(float u) {
+    const uint32_t ix = __float_as_uint(u) - 0x3F3504F3u;
+    const int k = (int)ix >> 23;
+    const float t = __fsub_rn(__uint_as_float((ix & 0x007FFFFFu) + 0x3F3504F3u), 1.0f);
+    float q = 0x1.321a4cp-3f;
+    q = __fmaf_rn(q, t, -0x1.068b2ap-2f);
+    q = __fmaf_rn(q, t, 0x1.0f9b0cp-2f);
+    q = __fmaf_rn(q, t, -0x1.22bf86p-2f);
+    q = __fmaf_rn(q, t, 0x1.5424e0p-2f);
+    q = __fmaf_rn(q, t, -0x1.999fc2p-2f);
+    q = __fmaf_rn(q, t, 0x1.000422p-1f);
+    q = __fmaf_rn(q, t, -0x1.555558p-1f);
+    q = __fmaf_rn(q, t, 0x1.fffff8p-1f);
+    const float r2 = __fmaf_rn(__fmul_rn(t, t), q, __fmul_rn(-2.0f, t));
+    return __fmaf_rn(__int2float_rn(k), -0x1.62e430p+0f, r2);
+}
+
 // sin and cos of 2 pi (2j+1) 2^-24 with j = w >> 9: the quadrant is removed in
-// integers, the remainder g in [-1/2, 1/2) quadrant goes through the Taylor
-// series of sin(pi g / 2) (to g^9) and cos(pi g / 2) (to g^10).
+// integers, the remainder g in [-1/2, 1/2) of a quadrant goes through
+// sin(pi g / 2) = g S(g^2) (to g^7) and cos(pi g / 2) = 1 + g^2 C(g^2) (to g^8),
+// S and C fitted by least squares on Chebyshev nodes (gen_sincos_poly.py;
+// at most 1e-7 absolute error in FP32).
 __device__ __forceinline__ void sincos_turn(uint32_t w, float& s, float& c) {
     const int32_t v = (int32_t)(((w >> 9) << 1) | 1u);
     const int32_t qv = (v + (1 << 21)) >> 22;
@@ -113,16 +137,14 @@ __device__ __forceinline__ void sincos_turn(uint32_t w, float& s, float& c) {
     const int q = qv & 3;
     const float g = __fmul_rn(__int2float_rn(r), 0x1p-22f);
     const float g2 = __fmul_rn(g, g);
-    float sp = 0x1.507834p-13f;
-    sp = __fmaf_rn(sp, g2, -0x1.32d2ccp-8f);
-    sp = __fmaf_rn(sp, g2, 0x1.466bc6p-4f);
-    sp = __fmaf_rn(sp, g2, -0x1.4abbcep-1f);
-    sp = __fmaf_rn(sp, g2, 0x1.921fb6p+0f);
+    float sp = -0x1.2cf598p-8f;
+    sp = __fmaf_rn(sp, g2, 0x1.465a3cp-4f);
+    sp = __fmaf_rn(sp, g2, -0x1.4abba8p-1f);
+    sp = __fmaf_rn(sp, g2, 0x1.921fb4p+0f);
     const float sa = __fmul_rn(g, sp);
-    float cp = -0x1.a6d1f2p-16f;
-    cp = __fmaf_rn(cp, g2, 0x1.e1f506p-11f);
-    cp = __fmaf_rn(cp, g2, -0x1.55d3c8p-6f);
-    cp = __fmaf_rn(cp, g2, 0x1.03c1f0p-2f);
+    float cp = 0x1.d9f188p-11f;
+    cp = __fmaf_rn(cp, g2, -0x1.55c64ap-6f);
+    cp = __fmaf_rn(cp, g2, 0x1.03c1dep-2f);
     cp = __fmaf_rn(cp, g2, -0x1.3bd3ccp+0f);
     const float ca = __fmaf_rn(cp, g2, 1.0f);
     const bool odd = q & 1, neg_s = q & 2, neg_c = (q == 1) || (q == 2);
@@ -137,11 +159,11 @@ __device__ __forceinline__ void sincos_turn(uint32_t w, float& s, float& c) {
 // read; the low bytes feed accept_word().
 __device__ __forceinline__ void normals3(uint4 w, float& n0, float& n1, float& n2) {
     float s, c;
-    const float r0 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.x))));
+    const float r0 = __fsqrt_rn(rad2_f(u01(w.x)));
     sincos_turn(w.y, s, c);
     n0 = __fmul_rn(r0, c);
     n1 = __fmul_rn(r0, s);
-    const float r1 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.z))));
+    const float r1 = __fsqrt_rn(rad2_f(u01(w.z)));
     sincos_turn(w.w, s, c);
     n2 = __fmul_rn(r1, c);
 }
@@ -150,11 +172,11 @@ __device__ __forceinline__ void normals3(uint4 w, float& n0, float& n1, float& n
 // (the first normal of the next, odd, bead).
 __device__ __forceinline__ void normals3_spare(uint4 w, float& n0, float& n1, float& n2, float& spare) {
     float s, c;
-    const float r0 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.x))));
+    const float r0 = __fsqrt_rn(rad2_f(u01(w.x)));
     sincos_turn(w.y, s, c);
     n0 = __fmul_rn(r0, c);
     n1 = __fmul_rn(r0, s);
-    const float r1 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.z))));
+    const float r1 = __fsqrt_rn(rad2_f(u01(w.z)));
     sincos_turn(w.w, s, c);
     n2 = __fmul_rn(r1, c);
     spare = __fmul_rn(r1, s);
@@ -164,7 +186,7 @@ __device__ __forceinline__ void normals3_spare(uint4 w, float& n0, float& n1, fl
 // not at hand.
 __device__ __forceinline__ float spare_of(uint4 wp) {
     float s, c;
-    const float r1 = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(wp.z))));
+    const float r1 = __fsqrt_rn(rad2_f(u01(wp.z)));
     sincos_turn(wp.w, s, c);
     return __fmul_rn(r1, s);
 }
@@ -173,7 +195,7 @@ __device__ __forceinline__ float spare_of(uint4 wp) {
 // (w.x, w.y) of its own block.  Three Box-Muller pairs per two beads.
 __device__ __forceinline__ void normals3_odd(float spare, uint4 w, float& n0, float& n1, float& n2) {
     float s, c;
-    const float r = __fsqrt_rn(__fmul_rn(-2.0f, log_f(u01(w.x))));
+    const float r = __fsqrt_rn(rad2_f(u01(w.x)));
     sincos_turn(w.y, s, c);
     n0 = spare;
     n1 = __fmul_rn(r, c);
@@ -189,12 +211,14 @@ __device__ __forceinline__ uint32_t accept_word(uint4 w) {
 // floor(x * inv_d) mod n, in [0, n), for |x * inv_d| < 2^22 (beyond that the
 // index stays in [0, n) but need not be the floor).  FP32 restatement of the
 // periodic fold in coord_to_index_unified_high (device_function.cu:313-360).
-// floor(t) for |t| < 2^22 without a conversion instruction: t + 1.5*2^23
-// rounded down is 1.5*2^23 + floor(t) exactly, read back from the mantissa.
+// floor(t) of the exact product t = x * inv_d, for |t| < 2^22, in one fused
+// multiply-add and no conversion instruction: x * inv_d + 1.5*2^23 rounded
+// down (once, __fmaf_rd) is 1.5*2^23 + floor(t) exactly, an integer-valued
+// float whose mantissa holds the floor.
 // One box away is folded with selects; the general modulo only runs for
 // coordinates more than one box length outside the primary box.
 __device__ __forceinline__ int fold(float x, float inv_d, int n) {
-    int i = __float_as_int(__fadd_rd(__fmul_rn(x, inv_d), 0x1.8p23f)) - 0x4B400000;
+    int i = __float_as_int(__fmaf_rd(x, inv_d, 0x1.8p23f)) - 0x4B400000;
     i = i < 0 ? i + n : i;
     i = i >= n ? i - n : i;
     if ((unsigned)i >= (unsigned)n) {
@@ -213,16 +237,16 @@ __device__ __forceinline__ int fold(float x, float inv_d, int n) {
 // such j and n).  Clamping j below 2^24 keeps every input, NaN included,
 // inside [0, n).  off and mag come from a table indexed by n.
 __device__ __forceinline__ int fold_magic(float x, float inv_d, int n, int off, uint32_t mag) {
-    uint32_t j = (uint32_t)(__float_as_int(__fadd_rd(__fmul_rn(x, inv_d), 0x1.8p23f)) - off);
+    uint32_t j = (uint32_t)(__float_as_int(__fmaf_rd(x, inv_d, 0x1.8p23f)) - off);
     j = min(j, 0x00FFFFFFu);
     return (int)(j - __umulhi(j, mag) * (uint32_t)n);
 }
 
 // The same fold for a power-of-two n: the low log2(n) bits of the mantissa
-// of t + 1.5*2^23 (rounded down) are floor(t) mod n, because 0x4B400000, the
+// of t + 1.5*2^23 (rounded down once) are floor(t) mod n, because 0x4B400000, the
 // offset of that mantissa, has no bits below 2^22.  Exact for |t| < 2^22.
 __device__ __forceinline__ int fold_pow2(float x, float inv_d, int mask) {
-    return __float_as_int(__fadd_rd(__fmul_rn(x, inv_d), 0x1.8p23f)) & mask;
+    return __float_as_int(__fmaf_rd(x, inv_d, 0x1.8p23f)) & mask;
 }
 
 }  // namespace scmf

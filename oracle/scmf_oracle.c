@@ -107,9 +107,31 @@ float orc_logf(float x) {
     return fmaf(fe, 0x1.62ep-1f, fmaf(fe, 0x1.0bfbe8p-15f, lm));
 }
 
+/* -2 ln u for u in (0, 1], the squared Box-Muller radius: u = 2^k m with m in
+ * [sqrt(1/2), sqrt(2)) from the bits of u minus those of sqrt(1/2), t = m - 1
+ * (exact), -2 log1p(t) = -2t + t^2 Q2(t) with Q2 = -2 Q of orc_logf (scaled
+ * exactly), plus k times -2 ln2 rounded to FP32. */
+float orc_rad2(float u) {
+    const uint32_t ix = f2u(u) - 0x3F3504F3u;
+    const int k = (int32_t)ix >> 23;
+    const float t = u2f((ix & 0x007FFFFFu) + 0x3F3504F3u) - 1.0f;
+    float q = 0x1.321a4cp-3f;
+    q = fmaf(q, t, -0x1.068b2ap-2f);
+    q = fmaf(q, t, 0x1.0f9b0cp-2f);
+    q = fmaf(q, t, -0x1.22bf86p-2f);
+    q = fmaf(q, t, 0x1.5424e0p-2f);
+    q = fmaf(q, t, -0x1.999fc2p-2f);
+    q = fmaf(q, t, 0x1.000422p-1f);
+    q = fmaf(q, t, -0x1.555558p-1f);
+    q = fmaf(q, t, 0x1.fffff8p-1f);
+    const float r2 = fmaf(t * t, q, -2.0f * t);
+    return fmaf((float)k, -0x1.62e430p+0f, r2);
+}
+
 /* sin and cos of the angle 2*pi*(2j+1)*2^-24, j = w >> 9.  The quadrant is
  * split off in integers, the remainder g in [-1/2, 1/2) of a quadrant goes
- * through the Taylor series of sin(pi g/2) (to g^9) and cos(pi g/2) (to g^10). */
+ * through sin(pi g/2) = g S(g^2) (to g^7) and cos(pi g/2) = 1 + g^2 C(g^2) (to
+ * g^8), the fits of new_arch_b200/csrc/gen_sincos_poly.py. */
 void orc_sincos_turn(uint32_t w, float* s, float* c) {
     int32_t v = (int32_t)(((w >> 9) << 1) | 1u);
     int32_t qv = (v + (1 << 21)) >> 22;
@@ -117,16 +139,14 @@ void orc_sincos_turn(uint32_t w, float* s, float* c) {
     int q = qv & 3;
     float g = (float)r * 0x1p-22f;
     float g2 = g * g;
-    float sp = 0x1.507834p-13f;
-    sp = fmaf(sp, g2, -0x1.32d2ccp-8f);
-    sp = fmaf(sp, g2, 0x1.466bc6p-4f);
-    sp = fmaf(sp, g2, -0x1.4abbcep-1f);
-    sp = fmaf(sp, g2, 0x1.921fb6p+0f);
+    float sp = -0x1.2cf598p-8f;
+    sp = fmaf(sp, g2, 0x1.465a3cp-4f);
+    sp = fmaf(sp, g2, -0x1.4abba8p-1f);
+    sp = fmaf(sp, g2, 0x1.921fb4p+0f);
     float sa = g * sp;
-    float cp = -0x1.a6d1f2p-16f;
-    cp = fmaf(cp, g2, 0x1.e1f506p-11f);
-    cp = fmaf(cp, g2, -0x1.55d3c8p-6f);
-    cp = fmaf(cp, g2, 0x1.03c1f0p-2f);
+    float cp = 0x1.d9f188p-11f;
+    cp = fmaf(cp, g2, -0x1.55c64ap-6f);
+    cp = fmaf(cp, g2, 0x1.03c1dep-2f);
     cp = fmaf(cp, g2, -0x1.3bd3ccp+0f);
     float ca = fmaf(cp, g2, 1.0f);
     switch (q) {
@@ -143,11 +163,11 @@ void orc_sincos_turn(uint32_t w, float* s, float* c) {
  * 8..31 of each word are read; the low bytes feed orc_accept_word(). */
 void orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2) {
     float s, c;
-    float r0 = sqrtf(-2.0f * orc_logf(orc_u01(w[0])));
+    float r0 = sqrtf(orc_rad2(orc_u01(w[0])));
     orc_sincos_turn(w[1], &s, &c);
     *n0 = r0 * c;
     *n1 = r0 * s;
-    float r1 = sqrtf(-2.0f * orc_logf(orc_u01(w[2])));
+    float r1 = sqrtf(orc_rad2(orc_u01(w[2])));
     orc_sincos_turn(w[3], &s, &c);
     *n2 = r1 * c;
 }
@@ -158,10 +178,10 @@ void orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2) {
  * Box-Muller pairs per two beads. */
 void orc_normals3_odd(const uint32_t wp[4], const uint32_t w[4], float* n0, float* n1, float* n2) {
     float s, c;
-    float rb = sqrtf(-2.0f * orc_logf(orc_u01(wp[2])));
+    float rb = sqrtf(orc_rad2(orc_u01(wp[2])));
     orc_sincos_turn(wp[3], &s, &c);
     *n0 = rb * s;
-    float r = sqrtf(-2.0f * orc_logf(orc_u01(w[0])));
+    float r = sqrtf(orc_rad2(orc_u01(w[0])));
     orc_sincos_turn(w[1], &s, &c);
     *n1 = r * c;
     *n2 = r * s;
@@ -175,10 +195,12 @@ uint32_t orc_accept_word(const uint32_t w[4]) {
 
 /* Periodic fold of one coordinate to a cell index in [0, n): floor(x/dx) mod n
  * (for |x/dx| < 2^22, the range the kernels support).  Restates
- * coord_to_index_unified_high (device_function.cu:313-360) in FP32. */
+ * coord_to_index_unified_high (device_function.cu:313-360): the floor of the
+ * exact product x * inv_d of the two FP32 values (exact in FP64), which the
+ * kernels read from one round-down fused multiply-add. */
 int orc_fold(float x, float inv_d, int n) {
-    float t = x * inv_d;
-    int i = (int)floorf(t);
+    double t = (double)x * (double)inv_d;
+    int i = (int)floor(t);
     if ((unsigned)i >= (unsigned)n) {
         i %= n;
         if (i < 0) i += n;
