@@ -335,6 +335,8 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t, cudaStream_t st) 
     one_seed_hi = p.one_seed_hi && !p.close.empty();
     seed = p.seed;
     n_sys = (int)p.close.size();
+    lean = n_sys == 1 && p.lean_ok && p.fold_kind == 0 && p.linear;
+    sc = p.sc;
     std::vector<int32_t> fl, wl;
     for (size_t i = 0; i < p.move.size(); ++i) (p.tile_flat[i] ? fl : wl).push_back((int32_t)i);
     n_flat = (int)fl.size();
@@ -380,6 +382,8 @@ LaunchShape DevPlan::move_shape() const {
     sh.flat_threads = flat_threads;
     sh.keyed = one_seed ? kKeysBoth : (one_seed_hi ? kKeysHigh : kKeysNone);
     sh.keys = philox_schedule((uint32_t)seed, (uint32_t)(seed >> 32));
+    sh.lean = lean && one_seed && n_flat == 0 ? 1 : 0;
+    sh.sc = sc;
     return sh;
 }
 
@@ -469,8 +473,32 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
     const size_t first_tile = p->move.size();
     const size_t first_field = p->field.size();
     p->fold_kind = std::max(p->fold_kind, fold_kind_of(spec));
+    // the lean kernel indexes beads and cells (times types) with 32-bit integers
+    p->lean_ok = p->lean_ok && n_beads < (1ll << 31) && (int64_t)n_cells * spec.n_types < (1ll << 31);
     if (p->close.empty()) {
         p->seed = spec.p.seed;
+        SysDev h{};
+        fill_sysdev_constants(spec, n_beads, &h);
+        SysConsts& c = p->sc;
+        c.x = x;
+        c.y = y;
+        c.z = z;
+        c.chain_id = chain_id;
+        c.omega = omega;
+        c.n_cells = h.n_cells;
+        c.k2 = h.k2;
+        c.A = h.A;
+        c.R = h.R;
+        c.inv_dx = h.inv_dx;
+        c.inv_dy = h.inv_dy;
+        c.inv_dz = h.inv_dz;
+        c.nx = h.nx;
+        c.ny = h.ny;
+        c.nz = h.nz;
+        for (int g = 0; g < 3; ++g) {
+            c.cdeg[g] = h.cdeg[g];
+            c.ac4deg[g] = h.ac4deg[g];
+        }
     } else {
         if (p->seed != spec.p.seed) p->one_seed = false;
         if ((p->seed >> 32) != (spec.p.seed >> 32)) p->one_seed_hi = false;
@@ -514,6 +542,7 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
             p->max_chains = std::max(p->max_chains, mt.n_chains);
         }
         p->max_length = std::max(p->max_length, A.length);
+        p->lean_ok = p->lean_ok && A.linear && A.length % 2 == 0 && A.length <= 64 && 32 % (A.length / 2) == 0;
         p->max_deg = std::max(p->max_deg, A.max_deg);
         p->linear = p->linear && A.linear;
     }

@@ -76,6 +76,8 @@ struct Plan {
     uint64_t seed = 0;      // the systems' seed when they all share one
     bool one_seed = true;   // every system appended so far has `seed`
     bool one_seed_hi = true;  // ... or at least its upper 32 bits
+    bool lean_ok = true;      // every architecture so far fits the lean move kernel
+    SysConsts sc{};           // move constants of the first system appended
 };
 
 struct DevPlan {
@@ -96,6 +98,8 @@ struct DevPlan {
     bool one_seed = false;     // every system of the plan has `seed`: move launches take its key schedule
     bool one_seed_hi = false;  // they share its upper 32 bits: the second key word's schedule
     uint64_t seed = 0;
+    bool lean = false;  // one system that fits the lean move kernel (LaunchShape::lean)
+    SysConsts sc{};
     scmf_tune tune{};
     cudaGraphExec_t graph = nullptr;
     cudaGraph_t graph_src = nullptr;

@@ -172,6 +172,22 @@ inline PhiloxKeys philox_schedule(uint32_t k0, uint32_t k1) {
 
 enum KeyMode { kKeysNone = 0, kKeysHigh = 1, kKeysBoth = 2 };
 
+// Move constants of the one system of a launch, passed by value so that the
+// single-system move kernel reads them from the parameter constant bank
+// (instruction operands) instead of loading them from SysDev into registers.
+// Fixed for the life of the system: device buffers and spec constants.
+struct SysConsts {
+    float* x;
+    float* y;
+    float* z;
+    const uint32_t* chain_id;
+    const float* omega;
+    int64_t n_cells;
+    float k2, A, R, inv_dx, inv_dy, inv_dz;
+    int32_t nx, ny, nz, pad;
+    float cdeg[3], ac4deg[3];  // c = 2k deg and A c / 4 for 0, 1, 2 bonds
+};
+
 struct LaunchShape {
     int blocks;    // 0 = one CTA per tile
     int threads;
@@ -193,6 +209,11 @@ struct LaunchShape {
     // `keys`, kKeysHigh when they share its upper 32 bits, else kKeysNone
     int keyed;
     PhiloxKeys keys;
+    // the launch moves one system (constants `sc`) whose architectures are all
+    // linear chains of an even length L <= 64 with L/2 dividing 32, on a grid of
+    // power-of-two axes, with fewer than 2^31 beads: the lean move kernel runs
+    int lean;
+    SysConsts sc;
 };
 
 // Streaming multiprocessors of the current device (read once per device; 148

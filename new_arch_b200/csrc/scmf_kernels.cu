@@ -8,6 +8,8 @@
 //                   its cell, so counts stay the grid of the positions
 //                   (device_function.cu:471-508); or, in kGridOnly, a gridding
 //                   pass from scratch
+//   k_sweep_lean    the same sweep for one system of even-length chains on a
+//                   power-of-two grid, constants in the parameter bank
 //   k_sweep_linear  the same for longer linear chains, staged per warp in
 //                   shared memory
 //   k_sweep         the same for any bond graph (graph-colour half-sweeps)
@@ -803,6 +805,165 @@ __global__ void __maxnreg__(reg_cap(ANY_FLAT, FOLD, KEYS)) k_sweep_reg(const Mov
     }
 }
 
+// Lean move kernel for launches of one system whose architectures are linear
+// chains of an even length L <= 64 with L/2 dividing 32, on a grid of
+// power-of-two axes (LaunchShape::lean; the large system and the blend are
+// such launches).  Same sweep, trials and random numbers as k_sweep_reg, with
+// less work per trial:
+//  * the system's constants (positions, omega, chain ids, k, A, R, cell
+//    inverses, grid, per-degree c and A c / 4) come from the parameter bank
+//    (SysConsts), the Philox round keys too;
+//  * every pair has an odd bead, so the even/odd branches go away; a missing
+//    bond neighbour at a chain end is replaced by the bead itself, whose term
+//    fma(+0, 2k, f) leaves the force bit for bit as if it were skipped (the
+//    force starts at +0 and can only be -0 from a -0 sum, which RN never
+//    gives here);
+//  * lanes beyond the tile's last chain (a partial last iteration) repeat the
+//    last chain and store nothing, so every lane runs the same code;
+//  * the Metropolis logarithm and the count moves sit under warp-uniform
+//    branches (__any_sync); the outcome of every trial is unchanged.
+// Bead and cell indices are 32-bit (the plan checks the sizes).
+__device__ __forceinline__ bool trial_lean(const MoveConsts& c, float x, float y, float z, float fx, float fy,
+                                           float fz, float cc, float ac4, float n0, float n1, float n2, uint32_t aw,
+                                           const float* __restrict__ w_t, float& px, float& py, float& pz,
+                                           int& cell_old, int& cell_new) {
+    const float A = c.A, R = c.R;
+    const float dx = __fmaf_rn(A, fx, __fmul_rn(R, n0));
+    const float dy = __fmaf_rn(A, fy, __fmul_rn(R, n1));
+    const float dz = __fmaf_rn(A, fz, __fmul_rn(R, n2));
+    px = __fadd_rn(x, dx);
+    py = __fadd_rn(y, dy);
+    pz = __fadd_rn(z, dz);
+    const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+    const float fd = __fmaf_rn(fx, dx, __fmaf_rn(fy, dy, __fmul_rn(fz, dz)));
+    const float deb = __fmul_rn(ac4, __fmaf_rn(cc, d2, __fmul_rn(-2.0f, fd)));
+    cell_old = cell_of<0>(c, x, y, z);
+    cell_new = cell_of<0>(c, px, py, pz);
+    const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + cell_new), __ldg(w_t + cell_old)), deb);
+    // accept if dE < 0; else if dE < 17 and log(u) < -dE (log_floor decides
+    // without the logarithm for all but ~1 % of trials; see trial_f)
+    bool acc = dE < 0.0f;
+    const float u = u01(aw);
+    const bool near = !acc && dE < 17.0f && -dE > log_floor(u);
+    if (__any_sync(0xffffffffu, near)) acc = acc || (near && log_f(u) < -dE);
+    return acc;
+}
+
+template <int MODE>
+__global__ void __maxnreg__(64) k_sweep_lean(const MoveTile* __restrict__ tiles, int n_tiles,
+                                             const PhiloxKeys keys, const SysConsts sc) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    MoveConsts c;
+    c.k = 0.0f;
+    c.k2 = sc.k2;
+    c.A = sc.A;
+    c.R = sc.R;
+    c.inv_dx = sc.inv_dx;
+    c.inv_dy = sc.inv_dy;
+    c.inv_dz = sc.inv_dz;
+    c.nx = sc.nx;
+    c.ny = sc.ny;
+    c.nz = sc.nz;
+    c.pow2 = true;
+    c.small = false;
+    for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
+        const MoveTile t = tiles[ti];
+        SysDev* S = t.sys;
+        if (S->step >= S->stop_step) continue;  // block-uniform
+        const uint32_t step = S->step + 1u;
+        const ArchDev* Ap = t.arch;
+        const int L = Ap->length;
+        const int tpc = L >> 1;                                   // threads per chain, divides 32
+        const int cs = (int)div_magic((uint32_t)lane, Ap->tpc_magic, tpc);
+        const int tt = lane - cs * tpc;                           // pair index in the chain
+        const int cpw = 32 / tpc;                                 // chains per warp iteration
+        const int be = 2 * tt, bo = be + 1;
+        const bool first = tt == 0, last = tt == tpc - 1;         // chain ends: one bond
+        const float cc_e = first ? sc.cdeg[1] : sc.cdeg[2], ac4_e = first ? sc.ac4deg[1] : sc.ac4deg[2];
+        const float cc_o = last ? sc.cdeg[1] : sc.cdeg[2], ac4_o = last ? sc.ac4deg[1] : sc.ac4deg[2];
+        const int toff_e = (int)__ldg(Ap->types + be) * (int)sc.n_cells;
+        const int toff_o = (int)__ldg(Ap->types + bo) * (int)sc.n_cells;
+        const int nch = t.n_chains;
+        unsigned nacc = 0;
+        for (int cbase = warp * cpw; cbase < nch; cbase += nwarps * cpw) {  // warp-uniform bounds
+            const int chain = cbase + cs;
+            const bool live = chain < nch;
+            const int chl = live ? chain : nch - 1;
+            const int g = (int)t.bead0 + chl * L + be;
+            const float2 vx = __ldcs(reinterpret_cast<const float2*>(sc.x + g));
+            const float2 vy = __ldcs(reinterpret_cast<const float2*>(sc.y + g));
+            const float2 vz = __ldcs(reinterpret_cast<const float2*>(sc.z + g));
+            const uint32_t gc = __ldg(sc.chain_id + t.chain0 + chl);
+            float xe = vx.x, xo = vx.y, ye = vy.x, yo = vy.y, ze = vz.x, zo = vz.y;
+            // even bead 2t: bonds to 2t-1 (lane - 1's odd bead; the bead itself at the chain start) and 2t+1
+            float lx = __shfl_up_sync(0xffffffffu, xo, 1);
+            float ly = __shfl_up_sync(0xffffffffu, yo, 1);
+            float lz = __shfl_up_sync(0xffffffffu, zo, 1);
+            lx = first ? xe : lx;
+            ly = first ? ye : ly;
+            lz = first ? ze : lz;
+            const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), keys);
+            const uint4 wo = philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys);
+            float n0, n1, n2, spare;
+            normals3_spare(w, n0, n1, n2, spare);
+            bool acc_e, mv_e;
+            int ce_old, ce_new;
+            {
+                float fx = __fmaf_rn(__fsub_rn(lx, xe), c.k2, 0.0f);
+                float fy = __fmaf_rn(__fsub_rn(ly, ye), c.k2, 0.0f);
+                float fz = __fmaf_rn(__fsub_rn(lz, ze), c.k2, 0.0f);
+                add_bond(c.k2, xe, ye, ze, xo, yo, zo, fx, fy, fz);
+                float px, py, pz;
+                acc_e = trial_lean(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), sc.omega + toff_e,
+                                   px, py, pz, ce_old, ce_new) &&
+                        live;
+                xe = acc_e ? px : xe;
+                ye = acc_e ? py : ye;
+                ze = acc_e ? pz : ze;
+                mv_e = acc_e && ce_new != ce_old;
+            }
+            // odd bead 2t+1: bonds to 2t (moved) and 2t+2 (lane + 1's moved even bead; the bead itself at the end)
+            float rx = __shfl_down_sync(0xffffffffu, xe, 1);
+            float ry = __shfl_down_sync(0xffffffffu, ye, 1);
+            float rz = __shfl_down_sync(0xffffffffu, ze, 1);
+            rx = last ? xo : rx;
+            ry = last ? yo : ry;
+            rz = last ? zo : rz;
+            normals3_odd(spare, wo, n0, n1, n2);
+            bool acc_o, mv_o;
+            int co_old, co_new;
+            {
+                float fx = __fmaf_rn(__fsub_rn(xe, xo), c.k2, 0.0f);
+                float fy = __fmaf_rn(__fsub_rn(ye, yo), c.k2, 0.0f);
+                float fz = __fmaf_rn(__fsub_rn(ze, zo), c.k2, 0.0f);
+                add_bond(c.k2, xo, yo, zo, rx, ry, rz, fx, fy, fz);
+                float px, py, pz;
+                acc_o = trial_lean(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), sc.omega + toff_o,
+                                   px, py, pz, co_old, co_new) &&
+                        live;
+                xo = acc_o ? px : xo;
+                yo = acc_o ? py : yo;
+                zo = acc_o ? pz : zo;
+                mv_o = acc_o && co_new != co_old;
+            }
+            nacc += (acc_e ? 1u : 0u) + (acc_o ? 1u : 0u);
+            if (MODE == kMoveGrid && __any_sync(0xffffffffu, mv_e || mv_o)) {
+                uint32_t* cnt = S->counts[S->cur];
+                const bool c16 = S->count16 != 0;
+                if (mv_e) count_move(cnt, c16, toff_e, ce_old, ce_new);
+                if (mv_o) count_move(cnt, c16, toff_o, co_old, co_new);
+            }
+            if (live) {
+                __stcs(reinterpret_cast<float2*>(sc.x + g), make_float2(xe, xo));
+                __stcs(reinterpret_cast<float2*>(sc.y + g), make_float2(ye, yo));
+                __stcs(reinterpret_cast<float2*>(sc.z + g), make_float2(ze, zo));
+            }
+        }
+        nacc = warp_sum(nacc);
+        if (lane == 0 && nacc) atomicAdd(&S->slot_acc[(ti * kMaxWarps + warp) % kSlots], (unsigned long long)nacc);
+    }
+}
+
 // ------------------------------------------------------------------ field
 
 // omega of one cell from its counts (NT = 0: runtime type count, up to
@@ -1388,6 +1549,12 @@ template <int MODE, bool FLAT>
 static void launch_reg(const LaunchShape& sh, int blocks, int threads, cudaStream_t st, const MoveTile* tiles,
                        const int32_t* list, int n, unsigned* acc) {
     const int keys = MODE == kGridOnly ? kKeysNone : sh.keyed;
+    if constexpr (MODE != kGridOnly && !FLAT) {
+        if (sh.lean && keys == kKeysBoth && sh.fold == 0 && !list) {
+            k_sweep_lean<MODE><<<blocks, threads, 0, st>>>(tiles, n, sh.keys, sh.sc);
+            return;
+        }
+    }
     if (keys == kKeysBoth) {
         if (sh.fold == 0)
             k_sweep_reg<MODE, FLAT, 0, kKeysBoth><<<blocks, threads, 0, st>>>(tiles, list, n, acc, sh.keys);
