@@ -822,7 +822,10 @@ __global__ void __maxnreg__(reg_cap(ANY_FLAT, FOLD, KEYS)) k_sweep_reg(const Mov
 //    last chain and store nothing, so every lane runs the same code;
 //  * the Metropolis logarithm and the count moves sit under warp-uniform
 //    branches (__any_sync); the outcome of every trial is unchanged.
-// Bead and cell indices are 32-bit (the plan checks the sizes).
+// Bead and cell indices are 32-bit (the plan checks the sizes).  Each warp
+// loads the next iteration's pairs while it moves the current ones; at 72
+// registers (seven 128-thread CTAs per SM) that took the large system's move
+// launch from 0.511 to 0.496 ms (0.513 ms at 64 registers without it).
 __device__ __forceinline__ bool trial_lean(const MoveConsts& c, float x, float y, float z, float fx, float fy,
                                            float fz, float cc, float ac4, float n0, float n1, float n2, uint32_t aw,
                                            const float* __restrict__ w_t, float& px, float& py, float& pz,
@@ -850,7 +853,7 @@ __device__ __forceinline__ bool trial_lean(const MoveConsts& c, float x, float y
 }
 
 template <int MODE>
-__global__ void __maxnreg__(64) k_sweep_lean(const MoveTile* __restrict__ tiles, int n_tiles,
+__global__ void __maxnreg__(72) k_sweep_lean(const MoveTile* __restrict__ tiles, int n_tiles,
                                              const PhiloxKeys keys, const SysConsts sc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     MoveConsts c;
@@ -884,16 +887,28 @@ __global__ void __maxnreg__(64) k_sweep_lean(const MoveTile* __restrict__ tiles,
         const int toff_e = (int)__ldg(Ap->types + be) * (int)sc.n_cells;
         const int toff_o = (int)__ldg(Ap->types + bo) * (int)sc.n_cells;
         const int nch = t.n_chains;
+        const int stride = nwarps * cpw;
         unsigned nacc = 0;
-        for (int cbase = warp * cpw; cbase < nch; cbase += nwarps * cpw) {  // warp-uniform bounds
+        // the pair and chain id of the next iteration are loaded one iteration
+        // ahead, so the DRAM latency overlaps this iteration's trials
+        float2 nvx = make_float2(0.0f, 0.0f), nvy = nvx, nvz = nvx;
+        uint32_t ngc = 0u;
+        auto fetch = [&](int cb) {
+            const int ch = min(cb + cs, nch - 1);
+            const int gn = (int)t.bead0 + ch * L + be;
+            nvx = __ldcs(reinterpret_cast<const float2*>(sc.x + gn));
+            nvy = __ldcs(reinterpret_cast<const float2*>(sc.y + gn));
+            nvz = __ldcs(reinterpret_cast<const float2*>(sc.z + gn));
+            ngc = __ldg(sc.chain_id + t.chain0 + ch);
+        };
+        if (warp * cpw < nch) fetch(warp * cpw);
+        for (int cbase = warp * cpw; cbase < nch; cbase += stride) {  // warp-uniform bounds
             const int chain = cbase + cs;
             const bool live = chain < nch;
-            const int chl = live ? chain : nch - 1;
-            const int g = (int)t.bead0 + chl * L + be;
-            const float2 vx = __ldcs(reinterpret_cast<const float2*>(sc.x + g));
-            const float2 vy = __ldcs(reinterpret_cast<const float2*>(sc.y + g));
-            const float2 vz = __ldcs(reinterpret_cast<const float2*>(sc.z + g));
-            const uint32_t gc = __ldg(sc.chain_id + t.chain0 + chl);
+            const int g = (int)t.bead0 + (live ? chain : nch - 1) * L + be;
+            const float2 vx = nvx, vy = nvy, vz = nvz;
+            const uint32_t gc = ngc;
+            if (cbase + stride < nch) fetch(cbase + stride);
             float xe = vx.x, xo = vx.y, ye = vy.x, yo = vy.y, ze = vz.x, zo = vz.y;
             // even bead 2t: bonds to 2t-1 (lane - 1's odd bead; the bead itself at the chain start) and 2t+1
             float lx = __shfl_up_sync(0xffffffffu, xo, 1);
