@@ -87,8 +87,14 @@ class System:
     def set_step(self, step: int) -> None:
         check(lib().scmf_set_step(self._h, int(step)))
 
-    def counts(self) -> np.ndarray:
-        out = np.empty(self.n_types * self.n_cells, dtype=np.uint32)
+    def counts(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Per-type cell counts [n_types * n_cells] (uint32), into `out` when
+        given (e.g. a view of page-locked memory, which copies fastest)."""
+        n = self.n_types * self.n_cells
+        if out is None:
+            out = np.empty(n, dtype=np.uint32)
+        if out.dtype != np.uint32 or out.size != n or not out.flags.c_contiguous:
+            raise ValueError(f"counts output must be a contiguous uint32 array of {n} elements")
         check(lib().scmf_get_counts(self._h, _ptr(out, C.c_uint32), out.size))
         return out
 
