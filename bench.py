@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["replicas", "sharded"], default="replicas",
+                    help="N GPUs: a replica of the large system per rank (default), or the large system's "
+                         "chains split over the ranks with an NCCL sum of the counts per sweep")
     ap.add_argument("--forms", choices=["all", "plain", "blend", "batched", "served"], default="all")
     ap.add_argument("--batched-sweeps", type=int, default=100)
     ap.add_argument("--served-requests", type=int, default=20000)
@@ -443,10 +446,63 @@ def run_capacity(nb, served_request, args):
             "wall_s": wall}
 
 
+def run_sharded(args):
+    """The large system as chain shards over the ranks (strong scaling): per
+    sweep each rank moves its chains, the counts are summed with one NCCL
+    all-reduce, and every rank computes the field of the sum."""
+    import datetime
+    import torch
+    from new_arch_b200.shard import ShardedSystem
+    from new_arch_b200.spec import large_system
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from new_arch_b200.replicas import reduce_max
+    spec = large_system(seed=7)
+    sh = ShardedSystem(spec)
+    sh.init_coords()
+    sh.step(args.warmup)
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    e0.record(st)
+    sh.step(args.steps)
+    e1.record(st)
+    e1.synchronize()
+    clocks = sampler.stop()
+    ms = reduce_max(e0.elapsed_time(e1), dist, "cuda")
+    cnt = sh.counts()
+    assert int(cnt.sum()) == spec.n_beads
+    sh.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {"metric": METRIC, "value": spec.n_beads * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (random-walk chains)",
+                "config": {"workload": WORKLOAD, "beads": spec.n_beads, "cells": spec.n_cells,
+                           "parallelism": f"chain shards x{world}, NCCL all-reduce of the counts per sweep",
+                           "l2": "inputs larger than L2 (614 MB coordinates), no flush"},
+                "clocks": clocks, "gpu_launches": 2 * args.steps * 1, "mode": "sharded"}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "sharded":
+        return run_sharded(args)
     return run_ours(args)
 
 

@@ -135,6 +135,32 @@ typedef struct scmf_stats {
 /* Allocates and owns all device memory of the system (initialize_structure_GPU,
  * init_config.cu:737-854).  cuda_stream may be NULL for a private stream. */
 scmf_status scmf_system_create(const scmf_spec* spec, void* cuda_stream, scmf_system** out);
+
+/* ---------------------------------------------------- chain shards (one system on several GPUs)
+ * The reference spreads one system's chains over GPUs (init_config.cu:220-222), sums the per-GPU
+ * int density counts by P2P copies and MPI_Allreduce (mesh.cu:10-81, mesh_mpi.cpp:16) and gives
+ * every GPU the summed field (mesh.cu:191-215).  A chain shard is that per-GPU part: chains
+ * [first[a], first[a] + count[a]) of every architecture a (scmf_shard_chains), each keeping the
+ * random stream of its id in the whole system, with the whole system's field scaling.  One sweep:
+ *   scmf_shard_move(shard, d_partial)        moves the shard's beads; its counts (the grid of its own
+ *                                            beads) are copied to d_partial
+ *   all-reduce (sum) of d_partial over the shards, by the caller (NCCL over NVLink, or any sum)
+ *   scmf_shard_field(shard, d_sum, 1)        omega of the summed counts (the same on every shard),
+ *                                            the field energy, and the close of the sweep
+ * After scmf_shard_init_coords(shard, d_partial) and the sum, scmf_shard_field(shard, d_sum, 0)
+ * computes the starting field.  Positions, summed counts and omega are bit-identical to the whole
+ * system's; accepted moves and bond energies are per shard (their sum is the system's).  Buffers
+ * are n_types * n_cells uint32 words in device memory; every call is enqueued on the shard's stream
+ * (order the caller's sum on that stream).  A shard refuses the whole-system step, init, coordinate,
+ * reference-shaped, batch and checkpoint calls, and needs 32-bit counts. */
+scmf_status scmf_system_create_shard(const scmf_spec* spec, int32_t shard, int32_t n_shards, void* cuda_stream,
+                                     scmf_system** out);
+/* first[a], count[a]: the chains of architecture a that shard `shard` of n_shards holds (host only). */
+scmf_status scmf_shard_chains(const scmf_spec* spec, int32_t shard, int32_t n_shards, int32_t* first, int32_t* count,
+                              int32_t n_arch);
+scmf_status scmf_shard_init_coords(scmf_system* shard, uint32_t* d_partial);
+scmf_status scmf_shard_move(scmf_system* shard, uint32_t* d_partial);
+scmf_status scmf_shard_field(scmf_system* shard, const uint32_t* d_total, int32_t close_sweep);
 /* A system that still belongs to a batch is freed when the last such batch is
  * destroyed; its handle must not be used after this call either way. */
 void scmf_system_destroy(scmf_system* sys);

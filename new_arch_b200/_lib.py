@@ -111,6 +111,11 @@ SIGNATURES = {
     "scmf_spec_copy": (_i32, [_vp, _pvp]),
     "scmf_spec_destroy": (None, [_vp]),
     "scmf_system_create": (_i32, [_vp, _vp, _pvp]),
+    "scmf_system_create_shard": (_i32, [_vp, _i32, _i32, _vp, _pvp]),
+    "scmf_shard_chains": (_i32, [_vp, _i32, _i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), _i32]),
+    "scmf_shard_init_coords": (_i32, [_vp, _vp]),
+    "scmf_shard_move": (_i32, [_vp, _vp]),
+    "scmf_shard_field": (_i32, [_vp, _vp, _i32]),
     "scmf_system_destroy": (None, [_vp]),
     "scmf_system_get_info": (_i32, [_vp, C.POINTER(SpecInfo)]),
     "scmf_system_stream": (_i32, [_vp, _pvp]),

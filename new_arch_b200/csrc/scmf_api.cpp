@@ -44,7 +44,7 @@ void free_system(scmf_system* s) {
     if (!s) return;
     s->plan.release();
     void* ptrs[] = {s->x, s->y, s->z, s->chain_id, s->counts[0], s->counts[1], s->omega, s->d_sys, s->d_arch,
-                    s->d_arch_blob, s->d_aos, s->d_u32, s->d_avg, s->d_ref, s->d_obs, s->d_check};
+                    s->d_arch_blob, s->d_aos, s->d_u32, s->d_avg, s->d_ref, s->d_obs, s->d_check, s->d_total};
     for (void* p : ptrs) dev_free(p, s->stream);
     if (s->own_stream && s->stream) {
         cudaStreamSynchronize(s->stream);
@@ -259,10 +259,28 @@ scmf_status scmf_debug_math(uint32_t key_lo, uint32_t key_hi, int32_t n, uint32_
 }
 
 // ---------------------------------------------------------------- system
-scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system** out) {
+// Chains [first[a], first[a] + count[a]) of each architecture a form chain shard
+// `shard` of `n_shards`: every architecture's chains are split into n_shards
+// contiguous, near-equal runs (the reference splits chains over GPUs the same
+// way, init_config.cu:220-222).
+static void shard_chains(const scmf_spec& spec, int shard, int n_shards, std::vector<int>* first,
+                         std::vector<int>* count) {
+    first->clear();
+    count->clear();
+    for (const auto& a : spec.archs) {
+        const int64_t lo = (int64_t)a.n_chains * shard / n_shards, hi = (int64_t)a.n_chains * (shard + 1) / n_shards;
+        first->push_back((int)lo);
+        count->push_back((int)(hi - lo));
+    }
+}
+
+static scmf_status create_system(const scmf_spec* spec, bool is_shard, int shard, int n_shards, void* stream,
+                                 scmf_system** out) {
     if (!spec || !out) return fail(SCMF_E_INVALID, "NULL argument");
     *out = nullptr;
     RET(validate_spec(*spec));
+    if (n_shards < 1 || shard < 0 || shard >= n_shards) return fail(SCMF_E_INVALID, "shard %d of %d", shard, n_shards);
+    if (is_shard && spec->p.count_bits != 32) return fail(SCMF_E_INVALID, "chain shards keep 32-bit counts");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
         cudaGetLastError();
@@ -271,11 +289,26 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
     if (int e = configure_kernels()) return fail(SCMF_E_CUDA, "kernel configuration: %s", cudaGetErrorString((cudaError_t)e));
     scmf_system* s = new scmf_system;
     s->spec = *spec;
+    s->is_shard = is_shard;
+    s->shard = shard;
+    s->n_shards = n_shards;
+    std::vector<int> first, count;
+    shard_chains(*spec, shard, n_shards, &first, &count);
+    int64_t whole_beads = 0;
+    for (size_t a = 0; a < spec->archs.size(); ++a) {
+        whole_beads += (int64_t)spec->archs[a].length * spec->archs[a].n_chains;
+        s->spec.archs[a].n_chains = count[a];
+    }
+    s->n_beads_total = whole_beads;
     scmf_status rc = prepare_archs(s->spec, &s->archs, &s->n_beads, &s->n_chains);
+    if (!rc && is_shard && s->n_beads == 0) rc = fail(SCMF_E_INVALID, "shard %d of %d holds no chains", shard, n_shards);
     if (rc) {
         delete s;
         return rc;
     }
+    // random-stream ids: a chain keeps the id it has in the whole system
+    for (size_t a = 0, base = 0; a < s->archs.size(); base += spec->archs[a].n_chains, ++a)
+        s->archs[a].rng_base = (int)base + first[a];
     s->n_cells = (int64_t)spec->nx * spec->ny * spec->nz;
     cudaGetDevice(&s->device);
     auto bail = [&](scmf_status r) {
@@ -298,7 +331,8 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
         (rc = dalloc(&s->counts[0], counts_bytes(s), &tot, st)) ||
         (rc = dalloc(&s->counts[1], counts_bytes(s), &tot, st)) || (rc = dalloc(&s->omega, cells_t * 4, &tot, st)) ||
         (rc = dalloc(&s->d_sys, sizeof(SysDev), &tot, st)) ||
-        (rc = dalloc(&s->d_arch, s->archs.size() * sizeof(ArchDev), &tot, st)))
+        (rc = dalloc(&s->d_arch, s->archs.size() * sizeof(ArchDev), &tot, st)) ||
+        (is_shard && (rc = dalloc(&s->d_total, cells_t * 4, &tot, st))))
         return bail(rc);
     // architecture tables
     size_t blob = 0;
@@ -330,6 +364,7 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
         d.tpc_magic = magic_for((uint32_t)((a.length + 1) / 2));
         d.n_chains = a.n_chains;
         d.chain_base = a.chain_base;
+        d.rng_base = a.rng_base;
         d.bead_base = a.bead_base;
         d.init_sigma = a.init_sigma;
         s->h_arch.push_back(d);
@@ -339,9 +374,12 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
             cudaSuccess)
         return bail(fail(SCMF_E_CUDA, "upload of architecture tables failed"));
     std::vector<uint32_t> ids(s->n_chains);
-    std::iota(ids.begin(), ids.end(), 0u);
+    for (const auto& a : s->archs)
+        for (int c = 0; c < a.n_chains; ++c) ids[a.chain_base + c] = (uint32_t)(a.rng_base + c);
     SysDev h{};
-    fill_sysdev_constants(s->spec, s->n_beads, &h);
+    fill_sysdev_constants(s->spec, s->n_beads_total, &h);  // field scaling n_cells / beads of the whole system
+    h.n_beads = s->n_beads;
+    h.field_counts = s->d_total;
     h.x = s->x; h.y = s->y; h.z = s->z;
     h.chain_id = s->chain_id;
     h.counts[0] = s->counts[0];
@@ -353,7 +391,8 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
         cudaMemsetAsync(s->z, 0, nbp * 4, st) != cudaSuccess ||
         cudaMemsetAsync(s->counts[0], 0, counts_bytes(s), st) != cudaSuccess ||
         cudaMemsetAsync(s->counts[1], 0, counts_bytes(s), st) != cudaSuccess ||
-        cudaMemsetAsync(s->omega, 0, cells_t * 4, st) != cudaSuccess)
+        cudaMemsetAsync(s->omega, 0, cells_t * 4, st) != cudaSuccess ||
+        (s->d_total && cudaMemsetAsync(s->d_total, 0, cells_t * 4, st) != cudaSuccess))
         return bail(fail(SCMF_E_CUDA, "initialisation of device buffers failed"));
     Plan p;
     const scmf_tune t = default_tune();
@@ -361,6 +400,62 @@ scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system*
     if ((rc = s->append_plan(t, &p)) || (rc = s->plan.upload(p, t, st))) return bail(rc);
     *out = s;
     return SCMF_OK;
+}
+
+scmf_status scmf_system_create(const scmf_spec* spec, void* stream, scmf_system** out) {
+    return create_system(spec, false, 0, 1, stream, out);
+}
+
+scmf_status scmf_system_create_shard(const scmf_spec* spec, int32_t shard, int32_t n_shards, void* stream,
+                                     scmf_system** out) {
+    return create_system(spec, true, shard, n_shards, stream, out);
+}
+
+scmf_status scmf_shard_chains(const scmf_spec* spec, int32_t shard, int32_t n_shards, int32_t* first,
+                              int32_t* count, int32_t n_arch) {
+    if (!spec || !first || !count) return fail(SCMF_E_INVALID, "NULL argument");
+    if (n_shards < 1 || shard < 0 || shard >= n_shards) return fail(SCMF_E_INVALID, "shard %d of %d", shard, n_shards);
+    if (n_arch != (int32_t)spec->archs.size()) return fail(SCMF_E_INVALID, "the spec has %zu architectures", spec->archs.size());
+    std::vector<int> f, c;
+    shard_chains(*spec, shard, n_shards, &f, &c);
+    for (int a = 0; a < n_arch; ++a) {
+        first[a] = f[a];
+        count[a] = c[a];
+    }
+    return SCMF_OK;
+}
+
+static scmf_status shard_only(const scmf_system* s) {
+    if (!s) return fail(SCMF_E_INVALID, "NULL system");
+    if (!s->is_shard) return fail(SCMF_E_STATE, "not a chain shard (scmf_system_create_shard)");
+    return SCMF_OK;
+}
+
+scmf_status scmf_shard_init_coords(scmf_system* s, uint32_t* d_partial) {
+    RET(shard_only(s));
+    if (!d_partial) return fail(SCMF_E_INVALID, "NULL counts buffer");
+    CKL(launch_init_coords(s->d_sys, s->d_arch, (int)s->archs.size(), s->n_chains, s->stream));
+    RET(regrid(s));
+    CKL(launch_copy_counts(s->d_sys, d_partial, s->n_cells * s->spec.n_types, s->stream));
+    return SCMF_OK;
+}
+
+scmf_status scmf_shard_move(scmf_system* s, uint32_t* d_partial) {
+    RET(shard_only(s));
+    if (!d_partial) return fail(SCMF_E_INVALID, "NULL counts buffer");
+    RET(fresh_counts(s));
+    RET(s->plan.enqueue_move(s->stream));
+    CKL(launch_copy_counts(s->d_sys, d_partial, s->n_cells * s->spec.n_types, s->stream));
+    return SCMF_OK;
+}
+
+scmf_status scmf_shard_field(scmf_system* s, const uint32_t* d_total, int32_t close_sweep) {
+    RET(shard_only(s));
+    if (!d_total) return fail(SCMF_E_INVALID, "NULL counts buffer");
+    CK(cudaMemcpyAsync(s->d_total, d_total, (size_t)s->n_cells * s->spec.n_types * 4, cudaMemcpyDeviceToDevice,
+                       s->stream));
+    if (close_sweep) return s->plan.enqueue_field(s->stream);
+    return field_now(s);
 }
 
 void scmf_system_destroy(scmf_system* s) {
@@ -385,6 +480,7 @@ scmf_status scmf_system_stream(const scmf_system* s, void** st) {
 }
 
 scmf_status scmf_init_coords(scmf_system* s) {
+    if (s && s->is_shard) return fail(SCMF_E_STATE, "a chain shard moves through scmf_shard_move / scmf_shard_field");
     if (!s) return fail(SCMF_E_INVALID, "NULL system");
     CKL(launch_init_coords(s->d_sys, s->d_arch, (int)s->archs.size(), s->n_chains, s->stream));
     RET(regrid(s));
@@ -394,6 +490,7 @@ scmf_status scmf_init_coords(scmf_system* s) {
 }
 
 scmf_status scmf_set_coords(scmf_system* s, const float* xyz, size_t n) {
+    if (s && s->is_shard) return fail(SCMF_E_STATE, "a chain shard moves through scmf_shard_move / scmf_shard_field");
     if (!s || !xyz) return fail(SCMF_E_INVALID, "NULL argument");
     if (n != (size_t)s->n_beads * 3) return fail(SCMF_E_INVALID, "expected %lld floats, got %zu", (long long)s->n_beads * 3, n);
     RET(ensure_aos(s));
@@ -426,6 +523,7 @@ scmf_status scmf_set_step(scmf_system* s, uint64_t step) {
 }
 
 scmf_status scmf_step_async(scmf_system* s, int32_t n) {
+    if (s && s->is_shard) return fail(SCMF_E_STATE, "a chain shard moves through scmf_shard_move / scmf_shard_field");
     if (!s || n < 0) return fail(SCMF_E_INVALID, "bad argument");
     RET(fresh_counts(s));
     return s->plan.run_sweeps(s->stream, n);
@@ -473,6 +571,7 @@ static scmf_status profile_sweeps(const DevPlan& p, cudaStream_t st, int32_t n, 
 }
 
 scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float* ms_field, float* ms_total) {
+    if (s && s->is_shard) return fail(SCMF_E_STATE, "a chain shard moves through scmf_shard_move / scmf_shard_field");
     if (!s || n < 0 || !ms_move || !ms_field || !ms_total) return fail(SCMF_E_INVALID, "bad argument");
     RET(fresh_counts(s));
     RET(profile_sweeps(s->plan, s->stream, n, ms_move, ms_field, ms_total));
@@ -480,6 +579,7 @@ scmf_status scmf_step_profiled(scmf_system* s, int32_t n, float* ms_move, float*
 }
 
 scmf_status scmf_smc_move(scmf_system* s, int32_t n) {
+    if (s && s->is_shard) return fail(SCMF_E_STATE, "a chain shard moves through scmf_shard_move / scmf_shard_field");
     if (!s || n < 0) return fail(SCMF_E_INVALID, "bad argument");
     const LaunchShape sh = s->plan.move_shape();
     for (int i = 0; i < n; ++i) {
@@ -493,6 +593,7 @@ scmf_status scmf_smc_move(scmf_system* s, int32_t n) {
 }
 
 scmf_status scmf_reset_density_fields(scmf_system* s) {
+    if (s && s->is_shard) return fail(SCMF_E_STATE, "a chain shard moves through scmf_shard_move / scmf_shard_field");
     if (!s) return fail(SCMF_E_INVALID, "NULL system");
     RET(regrid(s));
     CK(cudaStreamSynchronize(s->stream));
@@ -500,6 +601,7 @@ scmf_status scmf_reset_density_fields(scmf_system* s) {
 }
 
 scmf_status scmf_update_omega_fields_scmf0(scmf_system* s) {
+    if (s && s->is_shard) return fail(SCMF_E_STATE, "a chain shard moves through scmf_shard_move / scmf_shard_field");
     if (!s) return fail(SCMF_E_INVALID, "NULL system");
     RET(field_now(s));
     CK(cudaStreamSynchronize(s->stream));
@@ -567,6 +669,7 @@ scmf_status scmf_get_sweep_stats(const scmf_system* s, scmf_stats* o) {
 }
 
 scmf_status scmf_step_stats(scmf_system* s, int32_t n, scmf_stats* o) {
+    if (s && s->is_shard) return fail(SCMF_E_STATE, "a chain shard moves through scmf_shard_move / scmf_shard_field");
     if (!s || !o || n < 0) return fail(SCMF_E_INVALID, "bad argument");
     RET(fresh_counts(s));
     RET(s->plan.run_sweeps(s->stream, n));
@@ -585,6 +688,7 @@ scmf_status scmf_step_stats(scmf_system* s, int32_t n, scmf_stats* o) {
 }
 
 scmf_status scmf_step_stats_async(scmf_system* s, int32_t n, scmf_stats* host_out) {
+    if (s && s->is_shard) return fail(SCMF_E_STATE, "a chain shard moves through scmf_shard_move / scmf_shard_field");
     if (!s || !host_out || n < 0) return fail(SCMF_E_INVALID, "bad argument");
     RET(fresh_counts(s));
     RET(s->plan.run_sweeps(s->stream, n));
@@ -618,6 +722,8 @@ scmf_status scmf_get_stats(const scmf_system* cs, scmf_stats* o) {
 // --------------------------------------------------------------- batches
 scmf_status scmf_batch_create(scmf_system* const* systems, int32_t n, const scmf_tune* tune, void* stream,
                               scmf_batch** out) {
+    for (int32_t i = 0; systems && i < n; ++i)
+        if (systems[i] && systems[i]->is_shard) return fail(SCMF_E_STATE, "chain shards do not join batches");
     if (!systems || n < 1 || !out) return fail(SCMF_E_INVALID, "bad arguments");
     *out = nullptr;
     scmf_batch* b = new scmf_batch;

@@ -35,6 +35,7 @@ const char* last_error_cstr();
 // greedy colouring in index order, beads grouped by colour, division magics.
 struct ArchHost {
     int length = 0, n_colors = 0, n_chains = 0, chain_base = 0, max_deg = 0;
+    int rng_base = 0;  // random-stream id of the first chain (chain_base, or its id in the whole system)
     bool linear = false;  // bonds exactly (i, i+1): even/odd colouring, computed neighbours
     int64_t bead_base = 0;
     float init_sigma = 0;
@@ -130,11 +131,18 @@ scmf_tune resolve_tune(const scmf_tune* t);
 }  // namespace scmf
 
 struct scmf_system {
-    scmf_spec spec;
+    scmf_spec spec;  // for a chain shard: the shard's own chain counts
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int device = 0;
     int64_t n_beads = 0, n_cells = 0;
+    // chain shard `shard` of `n_shards` (n_shards == 1: a whole system); n_beads_total
+    // is the whole system's bead count (the field scaling), d_total the summed counts
+    // of all shards that its field step reads
+    bool is_shard = false;  // made by scmf_system_create_shard (any n_shards, 1 included)
+    int shard = 0, n_shards = 1;
+    int64_t n_beads_total = 0;
+    uint32_t* d_total = nullptr;
     int n_chains = 0;
     size_t device_bytes = 0;
     // device buffers

@@ -52,7 +52,9 @@ struct ArchDev {
     uint32_t len_magic;          // ceil(2^32 / length)
     uint32_t tpc_magic;          // magic of ceil(length / 2): threads per chain in k_sweep_reg
     int32_t n_chains;
-    int32_t chain_base;          // first global chain id of this architecture
+    int32_t chain_base;          // first storage slot of this architecture in the system
+    int32_t rng_base;            // random-stream id of its first chain: chain_base, or for a chain
+                                 // shard the id that chain has in the whole system
     int64_t bead_base;           // first bead of this architecture in the system arrays
     float init_sigma;
 };
@@ -97,6 +99,9 @@ struct SysDev {
     // round); 0xFFFFFFFF everywhere else
     uint32_t stop_step;
     uint32_t pad2;
+    // counts the field step reads: NULL means counts[cur] (the grid of this
+    // system's own beads); a chain shard points it at the sum over all shards
+    const uint32_t* field_counts;
     // the statistics of the last sweep in the public layout, written by
     // k_stats_out for asynchronous reads (scmf_step_stats_async)
     scmf_stats stats_out;
@@ -223,6 +228,8 @@ int sm_count();
 int launch_init_coords(SysDev* d_sys, const ArchDev* d_arch, int n_arch, int n_chains, void* stream);
 // Writes the statistics of the last sweep into d_sys->stats_out (one thread).
 int launch_stats_out(SysDev* d_sys, void* stream);
+// Copies the current counts (counts[cur], 32-bit words) into dst.
+int launch_copy_counts(const SysDev* d_sys, uint32_t* dst, int64_t n_words, void* stream);
 // Move kernels add their accept counts into SysDev::slot_acc (32-way spread);
 // the field kernel writes one energy per tile into ef_part, the bond-energy
 // kernel one per move tile into eb_part; k_close sums and publishes them.

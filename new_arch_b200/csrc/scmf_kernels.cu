@@ -50,6 +50,7 @@ __global__ void k_init_coords(SysDev* __restrict__ S, const ArchDev* __restrict_
     const ArchDev& A = archs[a];
     const int L = A.length;
     const int64_t b0 = A.bead_base + (int64_t)(g - A.chain_base) * L;
+    const uint32_t gid = (uint32_t)(A.rng_base + (g - A.chain_base));  // the chain's random-stream id
     float* X = S->x + b0;
     float* Y = S->y + b0;
     float* Z = S->z + b0;
@@ -61,7 +62,7 @@ __global__ void k_init_coords(SysDev* __restrict__ S, const ArchDev* __restrict_
         Y[i] = 0.0f;
         Z[i] = 0.0f;
     }
-    uint4 w = philox4x32_10(make_uint4((uint32_t)g, 0u, kInitStep, 0u), k0, k1);
+    uint4 w = philox4x32_10(make_uint4(gid, 0u, kInitStep, 0u), k0, k1);
     X[0] = u01(w.x) * S->lx;
     Y[0] = u01(w.y) * S->ly;
     Z[0] = u01(w.z) * S->lz;
@@ -72,7 +73,7 @@ __global__ void k_init_coords(SysDev* __restrict__ S, const ArchDev* __restrict_
             const int j = bi.nbr[d];
             if (placed[j >> 5] & (1u << (j & 31))) continue;
             float n0, n1, n2;
-            normals3(philox4x32_10(make_uint4((uint32_t)g, (uint32_t)j, kInitStep, 1u), k0, k1), n0, n1, n2);
+            normals3(philox4x32_10(make_uint4(gid, (uint32_t)j, kInitStep, 1u), k0, k1), n0, n1, n2);
             X[j] = X[i] + A.init_sigma * n0;
             Y[j] = Y[i] + A.init_sigma * n1;
             Z[j] = Z[i] + A.init_sigma * n2;
@@ -1165,7 +1166,7 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
         const float scale = S->scale;
         const bool lit = S->hamiltonian == 1;
         const bool c16 = S->count16 != 0;
-        const uint32_t* src32 = S->counts[cur];
+        const uint32_t* src32 = S->field_counts ? S->field_counts : S->counts[cur];
         float* W = S->omega;
         // the fused sweep samples the time-averaged density at every avg_every-th sweep
         unsigned long long* avg = FUSED && S->avg && S->avg_every && (sweep % S->avg_every) == 0u ? S->avg : nullptr;
@@ -1411,7 +1412,7 @@ __device__ __forceinline__ int64_t aos_bead_of(const SysDev* S, const ArchDev* a
     const int64_t slot_local = r / A.length;
     const int64_t b = r - slot_local * A.length;
     const uint32_t gc = S->chain_id[A.chain_base + slot_local];
-    return A.bead_base + (int64_t)(gc - (uint32_t)A.chain_base) * A.length + b;
+    return A.bead_base + (int64_t)(gc - (uint32_t)A.rng_base) * A.length + b;
 }
 
 __global__ void k_aos_to_soa(const float* __restrict__ aos, SysDev* S, const ArchDev* archs, int n_arch,
@@ -1501,6 +1502,17 @@ __global__ void k_stats_out(SysDev* S) {
     o.error_word = S->error_word;
     o.reserved = 0u;
     S->stats_out = o;
+}
+
+__global__ void k_copy_counts(const SysDev* __restrict__ S, uint32_t* __restrict__ dst, int64_t n) {
+    const uint32_t* src = S->counts[S->cur];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+int launch_copy_counts(const SysDev* d_sys, uint32_t* dst, int64_t n_words, void* stream) {
+    k_copy_counts<<<grid_for(n_words, 256), 256, 0, (cudaStream_t)stream>>>(d_sys, dst, n_words);
+    return (int)cudaGetLastError();
 }
 
 int launch_stats_out(SysDev* d_sys, void* stream) {

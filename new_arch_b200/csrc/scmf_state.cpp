@@ -277,6 +277,7 @@ scmf_status scmf_checkpoint_info(const char* path, scmf_checkpoint_header* out) 
 
 scmf_status scmf_checkpoint_read(scmf_system* s, const char* path) {
     if (!s || !path) return fail(SCMF_E_INVALID, "NULL argument");
+    if (s->is_shard) return fail(SCMF_E_STATE, "checkpoints hold whole systems, not chain shards");
     File f;
     f.f = fopen(path, "rb");
     if (!f.f) return fail(SCMF_E_IO, "cannot open %s: %s", path, strerror(errno));

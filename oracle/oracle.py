@@ -95,6 +95,8 @@ def lib():
     L.orc_normals3.argtypes = [u32p, f32p, f32p, f32p]
     L.orc_u01.restype = C.c_float
     L.orc_u01.argtypes = [C.c_uint32]
+    L.orc_set_shard.argtypes = [vp, C.POINTER(C.c_int), i64]
+    L.orc_field_from.argtypes = [vp, u32p]
     L.orc_trial_energy.restype = C.c_float
     L.orc_trial_energy.argtypes = [vp, i32, i32, f32p, f32p, f32p, C.c_float, C.c_float, C.c_float, f32p]
     L.orc_fold.restype = i32
@@ -231,6 +233,17 @@ class OracleSystem:
         out = np.zeros(self.n_types * self.n_cells, dtype=np.uint64)
         n = lib().orc_average_get(self._h, _p(out, C.c_uint64))
         return out, int(n)
+
+    def set_shard(self, rng_base, n_beads_total):
+        """Make this system a chain shard: rng_base[a] is the whole-system id of its
+        first chain of architecture a; the field scaling uses n_beads_total."""
+        a = np.ascontiguousarray(rng_base, dtype=np.int32)
+        lib().orc_set_shard(self._h, _p(a, C.c_int), int(n_beads_total))
+
+    def field_from(self, counts):
+        """omega and the field energy of the given counts (the sum over shards)."""
+        a = np.ascontiguousarray(counts, dtype=np.uint32)
+        lib().orc_field_from(self._h, _p(a, C.c_uint32))
 
     def trial_energy(self, arch, b, xyz, n):
         """(energy change, proposed position) of one trial of bead b of a chain of

@@ -212,6 +212,7 @@ int orc_fold(float x, float inv_d, int n) {
 
 typedef struct orc_arch {
     int length, n_chains, n_colors, chain_base;
+    int rng_base;       /* random-stream id of the first chain: chain_base, or its id in the whole system (shard) */
     int64_t bead_base;
     float init_sigma;
     int* type;          /* [length] */
@@ -320,6 +321,7 @@ int orc_finalize(orc_system* s) {
     for (int a = 0; a < s->n_arch; ++a) {
         s->arch[a].bead_base = nb;
         s->arch[a].chain_base = nc;
+        s->arch[a].rng_base = nc;
         nb += (int64_t)s->arch[a].length * s->arch[a].n_chains;
         nc += s->arch[a].n_chains;
     }
@@ -393,7 +395,7 @@ static inline void key_of(const orc_system* s, uint32_t key[2]) {
  * box, then every bead i in index order places each not-yet-placed neighbour
  * at pos[i] + sigma * N(0,1)^3. */
 static void init_chain(orc_system* s, const orc_arch* a, int ci, const uint32_t key[2], char* placed) {
-    uint32_t gc = (uint32_t)(a->chain_base + ci);
+    uint32_t gc = (uint32_t)(a->rng_base + ci);
     int64_t b0 = a->bead_base + (int64_t)ci * a->length;
     float* X = s->x + b0; float* Y = s->y + b0; float* Z = s->z + b0;
     uint32_t ctr[4] = {gc, 0u, ORC_INIT_STEP, 0u}, w[4];
@@ -590,7 +592,7 @@ static void sweep_moves(orc_system* s, uint32_t step) {
         for (int c = 0; c < ar->n_chains; ++c) {
             int64_t b0 = ar->bead_base + (int64_t)c * ar->length;
             float* X = s->x + b0; float* Y = s->y + b0; float* Z = s->z + b0;
-            uint32_t gc = (uint32_t)(ar->chain_base + c);
+            uint32_t gc = (uint32_t)(ar->rng_base + c);
             uint32_t nacc = 0;
             for (int col = 0; col < ar->n_colors; ++col)
                 for (int b = 0; b < ar->length; ++b)
@@ -634,7 +636,7 @@ void orc_reset_density(orc_system* s) {
 /* SCMF0 field (device_function.cu:373-412) in FP32, or the literal
  * omega_T = kappaN (sum phi - 1) + sum_{S!=T} chiN_TS phi_S per 1/N_ref
  * when hamiltonian == 1. */
-static void field_update(orc_system* s, int write_omega) {
+static void field_update_from(orc_system* s, const uint32_t* counts, int write_omega) {
     const int n = s->n_types;
     const int64_t nc = s->n_cells;
     double ef = 0.0;
@@ -642,7 +644,7 @@ static void field_update(orc_system* s, int write_omega) {
     for (int64_t c = 0; c < nc; ++c) {
         float phi[ORC_MAX_TYPES];
         float tot = 0.0f;
-        for (int u = 0; u < n; ++u) { phi[u] = (float)s->counts[u * nc + c] * s->scale; tot = tot + phi[u]; }
+        for (int u = 0; u < n; ++u) { phi[u] = (float)counts[u * nc + c] * s->scale; tot = tot + phi[u]; }
         for (int t = 0; t < n; ++t) {
             float w;
             if (write_omega) {
@@ -656,13 +658,26 @@ static void field_update(orc_system* s, int write_omega) {
             } else {
                 w = s->omega[t * nc + c];
             }
-            ef += (double)w * (double)s->counts[t * nc + c];
+            ef += (double)w * (double)counts[t * nc + c];
         }
     }
     s->st.e_field = ef;
 }
 
+static void field_update(orc_system* s, int write_omega) { field_update_from(s, s->counts, write_omega); }
+
 void orc_update_omega(orc_system* s) { field_update(s, 1); }
+
+/* Chain shard of a system (the reference's per-GPU chains, init_config.cu:220-222):
+ * rng_base[a] is the whole-system id of this system's first chain of
+ * architecture a, and the field scaling uses the whole system's bead count. */
+void orc_set_shard(orc_system* s, const int* rng_base, int64_t n_beads_total) {
+    for (int a = 0; a < s->n_arch; ++a) s->arch[a].rng_base = rng_base[a];
+    s->scale = n_beads_total > 0 ? (float)((double)s->n_cells / (double)n_beads_total) : 0.0f;
+}
+
+/* omega and the field energy of the given counts (the sum over all shards). */
+void orc_field_from(orc_system* s, const uint32_t* counts) { field_update_from(s, counts, 1); }
 
 /* One MC step per sweep, test.cpp:37-43: move, grid, then the field unless
  * the rule is "reference" and step % 10 == 0. */

@@ -104,6 +104,10 @@ float  orc_dE_closed(int deg, const float* q, const float* p, const float* d, fl
 /* energy change of one trial of bead b of a chain of architecture `arch`
  * (chain-local positions X, Y, Z) with the normals n0..n2; p_out[3] gets the
  * proposed position */
+/* chain shard: per-architecture random-stream bases and the whole system's bead count */
+void   orc_set_shard(orc_system* s, const int* rng_base, int64_t n_beads_total);
+/* omega (and field energy) of the given counts instead of the system's own */
+void   orc_field_from(orc_system* s, const uint32_t* counts);
 float  orc_trial_energy(const orc_system* s, int arch, int b, const float* X, const float* Y, const float* Z, float n0,
                         float n1, float n2, float* p_out);
 
