@@ -466,7 +466,7 @@ def run_sharded(args):
     sh = ShardedSystem(spec)
     sh.init_coords()
     sh.step(args.warmup)
-    st = torch.cuda.current_stream()
+    st = sh.stream
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist is not None:
         dist.barrier()

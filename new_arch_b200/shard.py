@@ -103,7 +103,8 @@ class Shard:
 class ShardedSystem:
     """This rank's shard of one system spread over the ranks of a
     torch.distributed process group (backend "nccl", one GPU per rank); the
-    per-sweep sum of the counts is an in-place all-reduce on the current stream."""
+    per-sweep sum of the counts is an in-place all-reduce on the shard's stream
+    (`stream`; time it with events recorded there)."""
 
     def __init__(self, spec: SystemSpec, group=None):
         import torch
@@ -114,13 +115,19 @@ class ShardedSystem:
         else:                       # one process, one shard: the sum is the shard's own counts
             rank, world = 0, 1
         self.world = world
-        self.stream = torch.cuda.current_stream()
+        # a stream of its own (never the legacy default stream, whose handle is 0,
+        # which the C ABI reads as "make a private stream"): the shard's kernels and
+        # the all-reduce are ordered on it
+        self._torch = torch
+        self.stream = torch.cuda.Stream()
         self.shard = Shard(spec, rank, world, self.stream.cuda_stream)
-        self.buf = torch.zeros(self.shard.count_words, dtype=torch.int32, device="cuda")
+        with torch.cuda.stream(self.stream):
+            self.buf = torch.zeros(self.shard.count_words, dtype=torch.int32, device="cuda")
 
     def _sum(self) -> None:
         if self.world > 1:
-            self._dist.all_reduce(self.buf, op=self._dist.ReduceOp.SUM, group=self._group)
+            with self._torch.cuda.stream(self.stream):
+                self._dist.all_reduce(self.buf, op=self._dist.ReduceOp.SUM, group=self._group)
 
     def init_coords(self) -> None:
         self.shard.init_coords(self.buf.data_ptr())

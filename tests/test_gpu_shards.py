@@ -33,20 +33,22 @@ def test_shards_equal_whole_system(name):
     from new_arch_b200.shard import Shard, shard_chains
     spec = _specs()[name]
     n_shards, sweeps = 3, 6
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()   # a real stream: handle 0 would give each shard a private one
     with nb.System(spec, stream=stream.cuda_stream) as whole:
         whole.init_coords()
         whole.step(sweeps)
         w_xyz, w_cnt, w_om, w_st = whole.coords(), whole.counts(), whole.omega(), whole.stats()
     shards = [Shard(spec, s, n_shards, stream.cuda_stream) for s in range(n_shards)]
     words = shards[0].count_words
-    part = [torch.zeros(words, dtype=torch.int32, device="cuda") for _ in shards]
-    total = torch.zeros(words, dtype=torch.int32, device="cuda")
+    with torch.cuda.stream(stream):
+        part = [torch.zeros(words, dtype=torch.int32, device="cuda") for _ in shards]
+        total = torch.zeros(words, dtype=torch.int32, device="cuda")
 
     def summed():
-        total.copy_(part[0])
-        for p in part[1:]:
-            total.add_(p)
+        with torch.cuda.stream(stream):
+            total.copy_(part[0])
+            for p in part[1:]:
+                total.add_(p)
 
     for sh, p in zip(shards, part):
         sh.init_coords(p.data_ptr())
@@ -70,7 +72,9 @@ def test_shards_equal_whole_system(name):
             pieces.append(xyz[starts[s]:starts[s] + n])
             starts[s] += n
     assert_coords_equal(np.concatenate(pieces), w_xyz, f"{name}: shard positions")
-    assert_counts_equal(total.cpu().numpy().view(np.uint32), w_cnt, f"{name}: summed counts")
+    with torch.cuda.stream(stream):
+        tot = total.cpu().numpy().view(np.uint32)
+    assert_counts_equal(tot, w_cnt, f"{name}: summed counts")
     acc = 0
     for sh in shards:
         assert np.array_equal(sh.omega().view(np.uint32), w_om.view(np.uint32)), f"{name}: shard omega"
