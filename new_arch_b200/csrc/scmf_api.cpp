@@ -46,6 +46,12 @@ void free_system(scmf_system* s) {
     void* ptrs[] = {s->x, s->y, s->z, s->chain_id, s->counts[0], s->counts[1], s->omega, s->d_sys, s->d_arch,
                     s->d_arch_blob, s->d_aos, s->d_u32, s->d_avg, s->d_ref, s->d_obs, s->d_check, s->d_total};
     for (void* p : ptrs) dev_free(p, s->stream);
+    if (s->copy_stream) {
+        cudaStreamSynchronize(s->copy_stream);
+        cudaStreamDestroy(s->copy_stream);
+        for (auto e : s->chunk_ev)
+            if (e) cudaEventDestroy(e);
+    }
     if (s->own_stream && s->stream) {
         cudaStreamSynchronize(s->stream);
         cudaStreamDestroy(s->stream);
@@ -489,14 +495,42 @@ scmf_status scmf_init_coords(scmf_system* s) {
     return check_error_word(s);
 }
 
+// Positions from host AoS in chunks: chunk k's host-to-device copy runs on the
+// copy stream while the system stream converts and grids chunk k - 1, so the
+// conversion and the gridding hide behind the transfer (the first sweep cannot:
+// its moves read the field of all the new positions).
+static scmf_status upload_chunked(scmf_system* s, const float* xyz) {
+    constexpr int kChunks = 8;
+    if (!s->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+        for (auto& e : s->chunk_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    CK(cudaMemsetAsync(s->counts[0], 0, counts_bytes(s), s->stream));
+    CK(cudaMemsetAsync(s->counts[1], 0, counts_bytes(s), s->stream));
+    CK(cudaMemsetAsync((char*)s->d_sys + offsetof(SysDev, cur), 0, sizeof(uint32_t), s->stream));
+    // the staging buffer is free once the system stream's earlier work is done
+    CK(cudaEventRecord(s->chunk_ev[0], s->stream));
+    CK(cudaStreamWaitEvent(s->copy_stream, s->chunk_ev[0], 0));
+    const int64_t n = s->n_beads, per = (n + kChunks - 1) / kChunks;
+    for (int k = 0; k < kChunks; ++k) {
+        const int64_t i0 = std::min<int64_t>(n, k * per), i1 = std::min<int64_t>(n, i0 + per);
+        if (i1 <= i0) break;
+        CK(cudaMemcpyAsync(s->d_aos + 3 * i0, xyz + 3 * i0, (size_t)(i1 - i0) * 3 * sizeof(float),
+                           cudaMemcpyHostToDevice, s->copy_stream));
+        CK(cudaEventRecord(s->chunk_ev[k], s->copy_stream));
+        CK(cudaStreamWaitEvent(s->stream, s->chunk_ev[k], 0));
+        CKL(launch_aos_chunk(s->d_aos, s->d_sys, s->d_arch, (int)s->archs.size(), i0, i1, s->stream));
+    }
+    s->counts_stale = false;
+    return SCMF_OK;
+}
+
 scmf_status scmf_set_coords(scmf_system* s, const float* xyz, size_t n) {
     if (s && s->is_shard) return fail(SCMF_E_STATE, "a chain shard moves through scmf_shard_move / scmf_shard_field");
     if (!s || !xyz) return fail(SCMF_E_INVALID, "NULL argument");
     if (n != (size_t)s->n_beads * 3) return fail(SCMF_E_INVALID, "expected %lld floats, got %zu", (long long)s->n_beads * 3, n);
     RET(ensure_aos(s));
-    CK(cudaMemcpyAsync(s->d_aos, xyz, n * sizeof(float), cudaMemcpyHostToDevice, s->stream));
-    CKL(launch_aos_to_soa(s->d_aos, s->d_sys, s->d_arch, (int)s->archs.size(), s->n_beads, s->stream));
-    RET(regrid(s));
+    RET(upload_chunked(s, xyz));
     RET(field_now(s));
     CK(cudaStreamSynchronize(s->stream));
     return check_error_word(s);

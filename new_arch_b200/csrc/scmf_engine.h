@@ -156,6 +156,9 @@ struct scmf_system {
     scmf::ArchDev* d_arch = nullptr;
     void* d_arch_blob = nullptr;
     float* d_aos = nullptr;      // staging for AoS coordinate transfers (lazy)
+    // chunked uploads: copies on their own stream, one event per chunk (lazy)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t chunk_ev[8] = {};
     uint32_t* d_u32 = nullptr;   // staging for unpacked 16-bit counts (lazy)
     unsigned long long* d_avg = nullptr;  // time-averaged density accumulator (while averaging)
     float* d_ref = nullptr;      // reference snapshot for displacements, SoA (lazy)

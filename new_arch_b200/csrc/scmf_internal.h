@@ -244,6 +244,11 @@ int launch_close(const SysClose* list, int n_sys, const unsigned* acc_part, int 
                  const double* ef_part, const double* eb_part, int mode, void* stream);
 int launch_aos_to_soa(const float* aos, SysDev* sys, const ArchDev* arch, int n_arch, int64_t n_beads,
                       void* stream);
+// Storage beads [i0, i1) from AoS positions (storage order = chain order: the
+// AoS bead of storage bead i is bead i), then their counts added into
+// counts[0] (a cleared buffer): one chunk of a chunked coordinate upload.
+int launch_aos_chunk(const float* aos, SysDev* sys, const ArchDev* arch, int n_arch, int64_t i0, int64_t i1,
+                     void* stream);
 int launch_soa_to_aos(float* aos, const SysDev* sys, const ArchDev* arch, int n_arch, int64_t n_beads,
                       void* stream);
 int launch_unpack_counts16(const SysDev* sys, uint32_t* out, int64_t n, void* stream);

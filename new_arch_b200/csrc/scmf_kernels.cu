@@ -1691,6 +1691,43 @@ int launch_close(const SysClose* list, int n_sys, const unsigned* acc_part, int 
     return (int)cudaGetLastError();
 }
 
+// One chunk of a chunked upload: positions of storage beads [i0, i1) (the
+// AoS bead of storage bead i is bead i: chain ids are the identity plus each
+// architecture's random-stream base) and their counts into counts[0].
+__global__ void k_aos_chunk(const float* __restrict__ aos, SysDev* S, const ArchDev* archs, int n_arch, int64_t i0,
+                            int64_t i1) {
+    MoveConsts c;
+    c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
+    c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
+    load_fold(c, S);
+    const int64_t NC = S->n_cells;
+    uint32_t* cnt = S->counts[0];
+    const bool c16 = S->count16 != 0;
+    for (int64_t i = i0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < i1; i += (int64_t)gridDim.x * blockDim.x) {
+        const float x = aos[3 * i], y = aos[3 * i + 1], z = aos[3 * i + 2];
+        S->x[i] = x;
+        S->y[i] = y;
+        S->z[i] = z;
+        int a = 0;
+        while (a + 1 < n_arch && i >= archs[a + 1].bead_base) ++a;
+        const ArchDev& A = archs[a];
+        const int r = (int)(i - A.bead_base);  // systems hold fewer than 2^31 beads
+        const int b = r % A.length;
+        const int64_t idx = (int64_t)A.types[b] * NC + cell_of(c, x, y, z);
+        if (c16)
+            atomicAdd(cnt + (idx >> 1), 1u << ((idx & 1) * 16));
+        else
+            atomicAdd(cnt + idx, 1u);
+    }
+}
+
+int launch_aos_chunk(const float* aos, SysDev* sys, const ArchDev* arch, int n_arch, int64_t i0, int64_t i1,
+                     void* stream) {
+    if (i1 <= i0) return 0;
+    k_aos_chunk<<<grid_for(i1 - i0, 256), 256, 0, (cudaStream_t)stream>>>(aos, sys, arch, n_arch, i0, i1);
+    return (int)cudaGetLastError();
+}
+
 int launch_aos_to_soa(const float* aos, SysDev* sys, const ArchDev* arch, int n_arch, int64_t n, void* stream) {
     if (n <= 0) return 0;
     k_aos_to_soa<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(aos, sys, arch, n_arch, n);
