@@ -336,6 +336,7 @@ scmf_status DevPlan::upload(const Plan& p, const scmf_tune& t, cudaStream_t st) 
     seed = p.seed;
     n_sys = (int)p.close.size();
     lean = n_sys == 1 && p.lean_ok && p.fold_kind == 0 && p.linear;
+    warp_even = p.warp_even && p.linear && p.max_length <= 64;
     sc = p.sc;
     std::vector<int32_t> fl, wl;
     for (size_t i = 0; i < p.move.size(); ++i) (p.tile_flat[i] ? fl : wl).push_back((int32_t)i);
@@ -383,6 +384,7 @@ LaunchShape DevPlan::move_shape() const {
     sh.keyed = one_seed ? kKeysBoth : (one_seed_hi ? kKeysHigh : kKeysNone);
     sh.keys = philox_schedule((uint32_t)seed, (uint32_t)(seed >> 32));
     sh.lean = lean && one_seed && n_flat == 0 ? 1 : 0;
+    sh.warp_even = warp_even ? 1 : 0;
     sh.sc = sc;
     return sh;
 }
@@ -543,6 +545,7 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
         }
         p->max_length = std::max(p->max_length, A.length);
         p->lean_ok = p->lean_ok && A.linear && A.length % 2 == 0 && A.length <= 64 && 32 % (A.length / 2) == 0;
+        if (A.linear && A.length <= 64 && 32 % ((A.length + 1) / 2) == 0) p->warp_even = p->warp_even && A.length % 2 == 0;
         p->max_deg = std::max(p->max_deg, A.max_deg);
         p->linear = p->linear && A.linear;
     }

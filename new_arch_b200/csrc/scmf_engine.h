@@ -78,6 +78,7 @@ struct Plan {
     bool one_seed = true;   // every system appended so far has `seed`
     bool one_seed_hi = true;  // ... or at least its upper 32 bits
     bool lean_ok = true;      // every architecture so far fits the lean move kernel
+    bool warp_even = true;    // every warp-wise linear architecture so far has an even length
     SysConsts sc{};           // move constants of the first system appended
 };
 
@@ -100,6 +101,7 @@ struct DevPlan {
     bool one_seed_hi = false;  // they share its upper 32 bits: the second key word's schedule
     uint64_t seed = 0;
     bool lean = false;  // one system that fits the lean move kernel (LaunchShape::lean)
+    bool warp_even = false;  // LaunchShape::warp_even
     SysConsts sc{};
     scmf_tune tune{};
     cudaGraphExec_t graph = nullptr;

@@ -219,6 +219,9 @@ struct LaunchShape {
     // power-of-two axes, with fewer than 2^31 beads: the lean move kernel runs
     int lean;
     SysConsts sc;
+    // every architecture whose chains fill warps exactly (ceil(L/2) divides 32)
+    // has an even length: those tiles run k_sweep_leanm
+    int warp_even;
 };
 
 // Streaming multiprocessors of the current device (read once per device; 148

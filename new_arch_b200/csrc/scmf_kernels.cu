@@ -10,6 +10,7 @@
 //                   pass from scratch
 //   k_sweep_lean    the same sweep for one system of even-length chains on a
 //                   power-of-two grid, constants in the parameter bank
+//   k_sweep_leanm   its structure for many systems / any grid (even lengths)
 //   k_sweep_linear  the same for longer linear chains, staged per warp in
 //                   shared memory
 //   k_sweep         the same for any bond graph (graph-colour half-sweeps)
@@ -980,6 +981,166 @@ __global__ void __maxnreg__(72) k_sweep_lean(const MoveTile* __restrict__ tiles,
     }
 }
 
+// The lean kernel's structure for launches of many systems (batches, served
+// rounds) and for single systems that k_sweep_lean does not take: linear chains
+// whose ceil(L/2) divides 32 with L even (LaunchShape::warp_even), any grid (FOLD
+// 0: every axis a power of two; -1: the fold is chosen per system) and any key
+// mode.  Each tile's system constants come from its SysDev into registers; at
+// 96 registers (no spill) the 256-system mix ran 7.39e10 bead-moves/s against
+// 7.00e10 with k_sweep_reg (80-88 registers spilled and lost).
+template <int FOLD>
+__device__ __forceinline__ bool trial_leanm(const MoveConsts& c, float x, float y, float z, float fx, float fy,
+                                           float fz, float cc, float ac4, float n0, float n1, float n2, uint32_t aw,
+                                           const float* __restrict__ w_t, float& px, float& py, float& pz,
+                                           int& cell_old, int& cell_new) {
+    const float A = c.A, R = c.R;
+    const float dx = __fmaf_rn(A, fx, __fmul_rn(R, n0));
+    const float dy = __fmaf_rn(A, fy, __fmul_rn(R, n1));
+    const float dz = __fmaf_rn(A, fz, __fmul_rn(R, n2));
+    px = __fadd_rn(x, dx);
+    py = __fadd_rn(y, dy);
+    pz = __fadd_rn(z, dz);
+    const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+    const float fd = __fmaf_rn(fx, dx, __fmaf_rn(fy, dy, __fmul_rn(fz, dz)));
+    const float deb = __fmul_rn(ac4, __fmaf_rn(cc, d2, __fmul_rn(-2.0f, fd)));
+    cell_old = cell_of<FOLD>(c, x, y, z);
+    cell_new = cell_of<FOLD>(c, px, py, pz);
+    const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + cell_new), __ldg(w_t + cell_old)), deb);
+    // accept if dE < 0; else if dE < 17 and log(u) < -dE (log_floor decides
+    // without the logarithm for all but ~1 % of trials; see trial_f)
+    bool acc = dE < 0.0f;
+    const float u = u01(aw);
+    const bool near = !acc && dE < 17.0f && -dE > log_floor(u);
+    if (__any_sync(0xffffffffu, near)) acc = acc || (near && log_f(u) < -dE);
+    return acc;
+}
+
+template <int MODE, int FOLD, int KEYS>
+__global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles, const int32_t* __restrict__ list, int n_list,
+                                             const PhiloxKeys keys) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int li = blockIdx.x; li < n_list; li += gridDim.x) {
+        const int ti = list ? __ldg(list + li) : li;
+        const MoveTile t = tiles[ti];
+        SysDev* S = t.sys;
+        if (S->step >= S->stop_step) continue;  // block-uniform
+        const uint32_t step = S->step + 1u;
+        MoveConsts c;
+        c.k = S->k; c.k2 = S->k2; c.A = S->A; c.R = S->R;
+        c.inv_dx = S->inv_dx; c.inv_dy = S->inv_dy; c.inv_dz = S->inv_dz;
+        load_fold(c, S);
+        const uint32_t k0 = S->seed_lo, k1 = S->seed_hi;
+        float* const PX = S->x;
+        float* const PY = S->y;
+        float* const PZ = S->z;
+        const uint32_t* const CID = S->chain_id;
+        const float* const OM = S->omega;
+        const int NCi = (int)S->n_cells;
+        const ArchDev* Ap = t.arch;
+        const int L = Ap->length;
+        const int tpc = L >> 1;                                   // threads per chain, divides 32
+        const int cs = (int)div_magic((uint32_t)lane, Ap->tpc_magic, tpc);
+        const int tt = lane - cs * tpc;                           // pair index in the chain
+        const int cpw = 32 / tpc;                                 // chains per warp iteration
+        const int be = 2 * tt, bo = be + 1;
+        const bool first = tt == 0, last = tt == tpc - 1;         // chain ends: one bond
+        const float cc_e = first ? S->cdeg[1] : S->cdeg[2], ac4_e = first ? S->ac4deg[1] : S->ac4deg[2];
+        const float cc_o = last ? S->cdeg[1] : S->cdeg[2], ac4_o = last ? S->ac4deg[1] : S->ac4deg[2];
+        const int toff_e = (int)__ldg(Ap->types + be) * NCi;
+        const int toff_o = (int)__ldg(Ap->types + bo) * NCi;
+        const int nch = t.n_chains;
+        const int stride = nwarps * cpw;
+        unsigned nacc = 0;
+        // the pair and chain id of the next iteration are loaded one iteration
+        // ahead, so the DRAM latency overlaps this iteration's trials
+        float2 nvx = make_float2(0.0f, 0.0f), nvy = nvx, nvz = nvx;
+        uint32_t ngc = 0u;
+        auto fetch = [&](int cb) {
+            const int ch = min(cb + cs, nch - 1);
+            const int gn = (int)t.bead0 + ch * L + be;
+            nvx = __ldcs(reinterpret_cast<const float2*>(PX + gn));
+            nvy = __ldcs(reinterpret_cast<const float2*>(PY + gn));
+            nvz = __ldcs(reinterpret_cast<const float2*>(PZ + gn));
+            ngc = __ldg(CID + t.chain0 + ch);
+        };
+        if (warp * cpw < nch) fetch(warp * cpw);
+        for (int cbase = warp * cpw; cbase < nch; cbase += stride) {  // warp-uniform bounds
+            const int chain = cbase + cs;
+            const bool live = chain < nch;
+            const int g = (int)t.bead0 + (live ? chain : nch - 1) * L + be;
+            const float2 vx = nvx, vy = nvy, vz = nvz;
+            const uint32_t gc = ngc;
+            if (cbase + stride < nch) fetch(cbase + stride);
+            float xe = vx.x, xo = vx.y, ye = vy.x, yo = vy.y, ze = vz.x, zo = vz.y;
+            // even bead 2t: bonds to 2t-1 (lane - 1's odd bead; the bead itself at the chain start) and 2t+1
+            float lx = __shfl_up_sync(0xffffffffu, xo, 1);
+            float ly = __shfl_up_sync(0xffffffffu, yo, 1);
+            float lz = __shfl_up_sync(0xffffffffu, zo, 1);
+            lx = first ? xe : lx;
+            ly = first ? ye : ly;
+            lz = first ? ze : lz;
+            const uint4 w = philox_block<KEYS>(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1, keys);
+            const uint4 wo = philox_block<KEYS>(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1, keys);
+            float n0, n1, n2, spare;
+            normals3_spare(w, n0, n1, n2, spare);
+            bool acc_e, mv_e;
+            int ce_old, ce_new;
+            {
+                float fx = __fmaf_rn(__fsub_rn(lx, xe), c.k2, 0.0f);
+                float fy = __fmaf_rn(__fsub_rn(ly, ye), c.k2, 0.0f);
+                float fz = __fmaf_rn(__fsub_rn(lz, ze), c.k2, 0.0f);
+                add_bond(c.k2, xe, ye, ze, xo, yo, zo, fx, fy, fz);
+                float px, py, pz;
+                acc_e = trial_leanm<FOLD>(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), OM + toff_e,
+                                   px, py, pz, ce_old, ce_new) &&
+                        live;
+                xe = acc_e ? px : xe;
+                ye = acc_e ? py : ye;
+                ze = acc_e ? pz : ze;
+                mv_e = acc_e && ce_new != ce_old;
+            }
+            // odd bead 2t+1: bonds to 2t (moved) and 2t+2 (lane + 1's moved even bead; the bead itself at the end)
+            float rx = __shfl_down_sync(0xffffffffu, xe, 1);
+            float ry = __shfl_down_sync(0xffffffffu, ye, 1);
+            float rz = __shfl_down_sync(0xffffffffu, ze, 1);
+            rx = last ? xo : rx;
+            ry = last ? yo : ry;
+            rz = last ? zo : rz;
+            normals3_odd(spare, wo, n0, n1, n2);
+            bool acc_o, mv_o;
+            int co_old, co_new;
+            {
+                float fx = __fmaf_rn(__fsub_rn(xe, xo), c.k2, 0.0f);
+                float fy = __fmaf_rn(__fsub_rn(ye, yo), c.k2, 0.0f);
+                float fz = __fmaf_rn(__fsub_rn(ze, zo), c.k2, 0.0f);
+                add_bond(c.k2, xo, yo, zo, rx, ry, rz, fx, fy, fz);
+                float px, py, pz;
+                acc_o = trial_leanm<FOLD>(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), OM + toff_o,
+                                   px, py, pz, co_old, co_new) &&
+                        live;
+                xo = acc_o ? px : xo;
+                yo = acc_o ? py : yo;
+                zo = acc_o ? pz : zo;
+                mv_o = acc_o && co_new != co_old;
+            }
+            nacc += (acc_e ? 1u : 0u) + (acc_o ? 1u : 0u);
+            if (MODE == kMoveGrid && __any_sync(0xffffffffu, mv_e || mv_o)) {
+                uint32_t* cnt = S->counts[S->cur];
+                const bool c16 = S->count16 != 0;
+                if (mv_e) count_move(cnt, c16, toff_e, ce_old, ce_new);
+                if (mv_o) count_move(cnt, c16, toff_o, co_old, co_new);
+            }
+            if (live) {
+                __stcs(reinterpret_cast<float2*>(PX + g), make_float2(xe, xo));
+                __stcs(reinterpret_cast<float2*>(PY + g), make_float2(ye, yo));
+                __stcs(reinterpret_cast<float2*>(PZ + g), make_float2(ze, zo));
+            }
+        }
+        nacc = warp_sum(nacc);
+        if (lane == 0 && nacc) atomicAdd(&S->slot_acc[(ti * kMaxWarps + warp) % kSlots], (unsigned long long)nacc);
+    }
+}
+
 // ------------------------------------------------------------------ field
 
 // omega of one cell from its counts (NT = 0: runtime type count, up to
@@ -1579,6 +1740,19 @@ static void launch_reg(const LaunchShape& sh, int blocks, int threads, cudaStrea
     if constexpr (MODE != kGridOnly && !FLAT) {
         if (sh.lean && keys == kKeysBoth && sh.fold == 0 && !list) {
             k_sweep_lean<MODE><<<blocks, threads, 0, st>>>(tiles, n, sh.keys, sh.sc);
+            return;
+        }
+        if (sh.warp_even) {
+            if (keys == kKeysBoth) {
+                if (sh.fold == 0) k_sweep_leanm<MODE, 0, kKeysBoth><<<blocks, threads, 0, st>>>(tiles, list, n, sh.keys);
+                else k_sweep_leanm<MODE, -1, kKeysBoth><<<blocks, threads, 0, st>>>(tiles, list, n, sh.keys);
+            } else if (keys == kKeysHigh) {
+                if (sh.fold == 0) k_sweep_leanm<MODE, 0, kKeysHigh><<<blocks, threads, 0, st>>>(tiles, list, n, sh.keys);
+                else k_sweep_leanm<MODE, -1, kKeysHigh><<<blocks, threads, 0, st>>>(tiles, list, n, sh.keys);
+            } else {
+                if (sh.fold == 0) k_sweep_leanm<MODE, 0, kKeysNone><<<blocks, threads, 0, st>>>(tiles, list, n, sh.keys);
+                else k_sweep_leanm<MODE, -1, kKeysNone><<<blocks, threads, 0, st>>>(tiles, list, n, sh.keys);
+            }
             return;
         }
     }

@@ -90,3 +90,35 @@ def test_lean_one_system_batch_with_explicit_tiles(nb):
         orc = oracle_for(spec)
         orc.step(5)
         compare_state(s, orc, "lean one-system batch")
+
+
+@pytest.mark.parametrize("seeds", ["one", "same_high_word", "distinct_high_words"])
+def test_leanm_batches_and_grids(nb, seeds):
+    """The multi-system lean kernel (k_sweep_leanm): systems of even,
+    warp-filling lengths on grids with and without power-of-two axes, batched
+    with each Philox key mode, plus a lone system on a grid that k_sweep_lean
+    does not take; a partial last iteration in every tile kind."""
+    specs = [nb.spec.diblock_melt(301, 16, 0.3, (10, 12, 7), 18.0, 50.0),
+             nb.spec.diblock_melt(157, 32, 0.6, (16, 16, 8), 25.0, 50.0),
+             nb.spec.diblock_melt(61, 64, 0.5, (9, 8, 11), 12.0, 50.0)]
+    for i, sp in enumerate(specs):
+        sp.seed = {"one": 5, "same_high_word": 5 + i, "distinct_high_words": 5 + (i << 33)}[seeds]
+    systems = [nb.System(sp) for sp in specs]
+    for s in systems:
+        s.init_coords()
+    b = nb.Batch(systems, tune={"threads_move": 64, "beads_per_tile": 1024})
+    b.step(5)
+    b.close()
+    for i, (sp, s) in enumerate(zip(specs, systems)):
+        orc = oracle_for(sp)
+        orc.step(5)
+        compare_state(s, orc, f"leanm {seeds} member {i}")
+        s.close()
+    # alone: one system, a grid without power-of-two axes
+    sp = nb.spec.diblock_melt(700, 32, 0.4, (12, 10, 14), 20.0, 50.0, seed=8)
+    with nb.System(sp) as s:
+        s.init_coords()
+        orc = oracle_for(sp)
+        s.step(6)
+        orc.step(6)
+        compare_state(s, orc, "leanm alone")
