@@ -212,12 +212,12 @@ scmf_status scmf_step_stats(scmf_system* sys, int32_t n_sweeps, scmf_stats* out)
 scmf_status scmf_step_stats_async(scmf_system* sys, int32_t n_sweeps, scmf_stats* host_out);
 
 /* Diagnostics: evaluates the device arithmetic (Philox4x32-10 with counter
- * (c0,c1,c2,c3) = (i, 0, 0, 0) and the given key, then log(u01(w.x)),
- * sin/cos of the angle of w.y and the three Box-Muller normals) for i < n on
- * the GPU, for comparison with any host restatement.  out must hold 8*n
- * floats: 4 raw words (as bits), log, sin, cos, normal0 per i; normals[3*n]. */
+ * (c0,c1,c2,c3) = (i, 0, 0, 0) and the given key, then log(u01(w.w)), the
+ * Metropolis logarithm, and the three inverse-CDF normals of w.x, w.y, w.z)
+ * for i < n on the GPU, for comparison with any host restatement.
+ * words[4*n] (raw), logs[n], normals[3*n]. */
 scmf_status scmf_debug_math(uint32_t key_lo, uint32_t key_hi, int32_t n, uint32_t* words, float* logs,
-                            float* sines, float* cosines, float* normals);
+                            float* normals);
 
 /* Field update that allocates nothing.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc: code that must not allocate while

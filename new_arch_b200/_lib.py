@@ -137,7 +137,7 @@ SIGNATURES = {
     "scmf_get_sweep_stats": (_i32, [_vp, C.POINTER(Stats)]),
     "scmf_step_stats": (_i32, [_vp, _i32, C.POINTER(Stats)]),
     "scmf_step_stats_async": (_i32, [_vp, _i32, _vp]),
-    "scmf_debug_math": (_i32, [_u32, _u32, _i32, _pu32, _pf32, _pf32, _pf32, _pf32]),
+    "scmf_debug_math": (_i32, [_u32, _u32, _i32, _pu32, _pf32, _pf32]),
     "scmf_update_omega_noalloc": (_i32, [_vp, _vp, _i32, _i64, _f64, _pf64, _i32, _i32, _vp, _vp]),
     "scmf_write_density": (_i32, [_vp, C.c_char_p, _i64]),
     "scmf_write_coords": (_i32, [_vp, C.c_char_p]),

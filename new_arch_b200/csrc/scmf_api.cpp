@@ -238,25 +238,21 @@ scmf_status scmf_spec_copy(const scmf_spec* s, scmf_spec** out) {
 
 void scmf_spec_destroy(scmf_spec* s) { delete s; }
 
-scmf_status scmf_debug_math(uint32_t key_lo, uint32_t key_hi, int32_t n, uint32_t* words, float* logs, float* sines,
-                            float* cosines, float* normals) {
-    if (n < 0 || !words || !logs || !sines || !cosines || !normals) return fail(SCMF_E_INVALID, "bad arguments");
+scmf_status scmf_debug_math(uint32_t key_lo, uint32_t key_hi, int32_t n, uint32_t* words, float* logs,
+                            float* normals) {
+    if (n < 0 || !words || !logs || !normals) return fail(SCMF_E_INVALID, "bad arguments");
     if (n == 0) return SCMF_OK;
     void* d = nullptr;
-    const size_t bytes = (size_t)n * (4 * 4 + 3 * 4 + 3 * 4);
+    const size_t bytes = (size_t)n * (4 * 4 + 4 + 3 * 4);
     CK(cudaMalloc(&d, bytes));
     uint32_t* dw = (uint32_t*)d;
     float* dl = (float*)(dw + 4 * (size_t)n);
-    float* ds = dl + n;
-    float* dc = ds + n;
-    float* dn = dc + n;
-    int e = launch_debug_math(key_lo, key_hi, n, dw, dl, ds, dc, dn, nullptr);
+    float* dn = dl + n;
+    int e = launch_debug_math(key_lo, key_hi, n, dw, dl, dn, nullptr);
     if (e == 0) e = (int)cudaDeviceSynchronize();
     if (e == 0) {
         cudaMemcpy(words, dw, 16 * (size_t)n, cudaMemcpyDeviceToHost);
         cudaMemcpy(logs, dl, 4 * (size_t)n, cudaMemcpyDeviceToHost);
-        cudaMemcpy(sines, ds, 4 * (size_t)n, cudaMemcpyDeviceToHost);
-        cudaMemcpy(cosines, dc, 4 * (size_t)n, cudaMemcpyDeviceToHost);
         cudaMemcpy(normals, dn, 12 * (size_t)n, cudaMemcpyDeviceToHost);
     }
     cudaFree(d);

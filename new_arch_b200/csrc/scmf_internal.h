@@ -274,7 +274,6 @@ void field_coefficients(int n, const double* xn, int nref, int hamiltonian, floa
 // Sets the thread's last-error message (scmf_engine.cpp); returns code.
 scmf_status fail(scmf_status code, const char* fmt, ...);
 int configure_kernels();
-int launch_debug_math(uint32_t k0, uint32_t k1, int n, uint32_t* words, float* logs, float* sines, float* cosines,
-                      float* normals, void* stream);
+int launch_debug_math(uint32_t k0, uint32_t k1, int n, uint32_t* words, float* logs, float* normals, void* stream);
 
 }  // namespace scmf

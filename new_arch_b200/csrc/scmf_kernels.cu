@@ -33,8 +33,21 @@
 
 #include "scmf_internal.h"
 #include "scmf_math.cuh"
+#include "scmf_normal_table.h"
 
 namespace scmf {
+
+// The inverse normal CDF table of normal_of, read-only in global memory.
+__device__ __align__(16) const float g_normal_tab[SCMF_NORMAL_SEGS * 4] = {SCMF_NORMAL_TABLE_DATA};
+
+__device__ __forceinline__ const float4* normal_table() { return reinterpret_cast<const float4*>(g_normal_tab); }
+
+// Copies the table into a block's shared memory (all threads of the block
+// call it; a barrier follows).
+__device__ __forceinline__ void load_normal_table(float4* s_tab) {
+    for (int i = threadIdx.x; i < SCMF_NORMAL_SEGS; i += blockDim.x) s_tab[i] = __ldg(normal_table() + i);
+    __syncthreads();
+}
 
 // i / n via a multiply-high by magic = ceil(2^32 / n) (exact while i * n < 2^32).
 __device__ __forceinline__ uint32_t div_magic(uint32_t i, uint32_t magic, int n) {
@@ -74,7 +87,7 @@ __global__ void k_init_coords(SysDev* __restrict__ S, const ArchDev* __restrict_
             const int j = bi.nbr[d];
             if (placed[j >> 5] & (1u << (j & 31))) continue;
             float n0, n1, n2;
-            normals3(philox4x32_10(make_uint4(gid, (uint32_t)j, kInitStep, 1u), k0, k1), n0, n1, n2);
+            normals3(philox4x32_10(make_uint4(gid, (uint32_t)j, kInitStep, 1u), k0, k1), normal_table(), n0, n1, n2);
             X[j] = X[i] + A.init_sigma * n0;
             Y[j] = Y[i] + A.init_sigma * n1;
             Z[j] = Z[i] + A.init_sigma * n2;
@@ -215,18 +228,12 @@ __device__ __forceinline__ uint4 philox_block(uint4 ctr, uint32_t k0, uint32_t k
     return philox4x32_10(ctr, k0, k1);
 }
 
-// Philox block and normals of bead b of chain gc (odd beads also draw the
-// block of b-1 for its spare sine).
+// Philox block and normals of bead b of chain gc; returns its Metropolis word.
 template <int KEYS>
 __device__ __forceinline__ uint32_t bead_normals(uint32_t gc, int b, uint32_t step, uint32_t k0, uint32_t k1,
                                                  const PhiloxKeys& keys, float& n0, float& n1, float& n2) {
     const uint4 w = philox_block<KEYS>(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1, keys);
-    if (b & 1) {
-        const float sp = spare_of(philox_block<KEYS>(make_uint4(gc, (uint32_t)(b - 1), step, 0u), k0, k1, keys));
-        normals3_odd(sp, w, n0, n1, n2);
-    } else {
-        normals3(w, n0, n1, n2);
-    }
+    normals3(w, normal_table(), n0, n1, n2);
     return accept_word(w);
 }
 
@@ -440,13 +447,10 @@ __global__ void __launch_bounds__(256, 3) k_sweep_linear(const MoveTile* __restr
                                                           const PhiloxKeys keys) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    // per warp: x, y, z of its chains (parity-split), then the spare sine of
-    // every even bead's block, which its odd partner takes as first normal
-    const int spare_len = (warp_beads + 1) / 2;
-    float* sx = reinterpret_cast<float*>(smem_raw) + (size_t)warp * (3 * warp_beads + spare_len);
+    // per warp: x, y, z of its chains (parity-split)
+    float* sx = reinterpret_cast<float*>(smem_raw) + (size_t)warp * 3 * warp_beads;
     float* sy = sx + warp_beads;
     float* sz = sy + warp_beads;
-    float* ssp = sz + warp_beads;
     for (int li = blockIdx.x; li < n_list; li += gridDim.x) {
         const int ti = list ? __ldg(list + li) : li;
         const MoveTile t = tiles[ti];
@@ -532,15 +536,7 @@ __global__ void __launch_bounds__(256, 3) k_sweep_linear(const MoveTile* __restr
                     }
                     const int type = __ldg(types + b);
                     float n0, n1, n2;
-                    const uint4 w = philox_block<KEYS>(make_uint4(gc, (uint32_t)b, step, 0u), k0, k1, keys);
-                    if (col == 0) {
-                        float sp;
-                        normals3_spare(w, n0, n1, n2, sp);
-                        ssp[cl * h0 + k] = sp;                  // for odd bead b + 1
-                    } else {
-                        normals3_odd(ssp[cl * h0 + k], w, n0, n1, n2);  // spare of even bead b - 1
-                    }
-                    const uint32_t aw = accept_word(w);
+                    const uint32_t aw = bead_normals<KEYS>(gc, b, step, k0, k1, keys, n0, n1, n2);
                     float px, py, pz;
                     int c_old, c_new;
                     const bool acc = trial<2>(c, sx[me], sy[me], sz[me], qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
@@ -615,6 +611,8 @@ __global__ void __maxnreg__(reg_cap(ANY_FLAT, FOLD, KEYS)) k_sweep_reg(const Mov
     // iteration parity: with one barrier per iteration a warp may write the
     // next iteration's slot while its left neighbour still reads this one
     __shared__ float s_first_even[2][kMaxWarps][3];
+    __shared__ float4 s_ntab[SCMF_NORMAL_SEGS];
+    if (MODE != kGridOnly) load_normal_table(s_ntab);
     // Every instance computes the odd bead's Philox block together with the
     // even bead's (two independent chains of rounds to interleave).  The keyed
     // instances, whose Philox key lives (at least half) in the parameter bank,
@@ -692,8 +690,7 @@ __global__ void __maxnreg__(reg_cap(ANY_FLAT, FOLD, KEYS)) k_sweep_reg(const Mov
                 }
                 continue;
             }
-            float spare = 0.0f;  // spare sine of the even bead's block, first normal of the odd bead
-            uint32_t wo_x = 0u, wo_y = 0u, wo_a = 0u;  // the odd bead's words (Box-Muller pair, accept)
+            uint4 wo = make_uint4(0u, 0u, 0u, 0u);  // the odd bead's Philox block
             // even half-sweep
             {
                 float lx = __shfl_up_sync(0xffffffffu, xo, 1);
@@ -723,14 +720,9 @@ __global__ void __maxnreg__(reg_cap(ANY_FLAT, FOLD, KEYS)) k_sweep_reg(const Mov
                         if (has_o) { qx[deg] = xo; qy[deg] = yo; qz[deg] = zo; ++deg; }
                     }
                     const uint4 w = philox_block<KEYS>(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1, keys);
-                    {
-                        const uint4 wo = philox_block<KEYS>(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1, keys);
-                        wo_x = wo.x;
-                        wo_y = wo.y;
-                        wo_a = accept_word(wo);
-                    }
+                    wo = philox_block<KEYS>(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1, keys);
                     float n0, n1, n2;
-                    normals3_spare(w, n0, n1, n2, spare);
+                    normals3(w, s_ntab, n0, n1, n2);
                     float px, py, pz;
                     int c_old, c_new;
                     const float cc = deg == 2 ? cc2 : (deg == 1 ? cc1 : 0.0f);
@@ -771,11 +763,11 @@ __global__ void __maxnreg__(reg_cap(ANY_FLAT, FOLD, KEYS)) k_sweep_reg(const Mov
                     int deg = 1;
                     if (bo + 1 < L) { qx[1] = rx; qy[1] = ry; qz[1] = rz; deg = 2; }
                     float n0, n1, n2;
-                    normals3_odd(spare, make_uint4(wo_x, wo_y, 0u, 0u), n0, n1, n2);
+                    normals3(wo, s_ntab, n0, n1, n2);
                     float px, py, pz;
                     int c_old, c_new;
                     const bool acc = trial<2, FOLD>(c, xo, yo, zo, qx, qy, qz, deg, deg == 2 ? cc2 : cc1,
-                                              deg == 2 ? ac42 : ac41, n0, n1, n2, wo_a,
+                                              deg == 2 ? ac42 : ac41, n0, n1, n2, accept_word(wo),
                                               omega + (int64_t)type_o * NC, px, py, pz, c_old, c_new);
                     if (acc) { xo = px; yo = py; zo = pz; }
                     nacc += acc ? 1u : 0u;
@@ -857,6 +849,8 @@ __device__ __forceinline__ bool trial_lean(const MoveConsts& c, float x, float y
 template <int MODE>
 __global__ void __maxnreg__(72) k_sweep_lean(const MoveTile* __restrict__ tiles, int n_tiles,
                                              const PhiloxKeys keys, const SysConsts sc) {
+    __shared__ float4 s_ntab[SCMF_NORMAL_SEGS];
+    load_normal_table(s_ntab);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     MoveConsts c;
     c.k = 0.0f;
@@ -921,8 +915,8 @@ __global__ void __maxnreg__(72) k_sweep_lean(const MoveTile* __restrict__ tiles,
             lz = first ? ze : lz;
             const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), keys);
             const uint4 wo = philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys);
-            float n0, n1, n2, spare;
-            normals3_spare(w, n0, n1, n2, spare);
+            float n0, n1, n2;
+            normals3(w, s_ntab, n0, n1, n2);
             bool acc_e, mv_e;
             int ce_old, ce_new;
             {
@@ -946,7 +940,7 @@ __global__ void __maxnreg__(72) k_sweep_lean(const MoveTile* __restrict__ tiles,
             rx = last ? xo : rx;
             ry = last ? yo : ry;
             rz = last ? zo : rz;
-            normals3_odd(spare, wo, n0, n1, n2);
+            normals3(wo, s_ntab, n0, n1, n2);
             bool acc_o, mv_o;
             int co_old, co_new;
             {
@@ -1018,6 +1012,8 @@ __device__ __forceinline__ bool trial_leanm(const MoveConsts& c, float x, float 
 template <int MODE, int FOLD, int KEYS>
 __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles, const int32_t* __restrict__ list, int n_list,
                                              const PhiloxKeys keys) {
+    __shared__ float4 s_ntab[SCMF_NORMAL_SEGS];
+    load_normal_table(s_ntab);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int li = blockIdx.x; li < n_list; li += gridDim.x) {
         const int ti = list ? __ldg(list + li) : li;
@@ -1081,8 +1077,8 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
             lz = first ? ze : lz;
             const uint4 w = philox_block<KEYS>(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1, keys);
             const uint4 wo = philox_block<KEYS>(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1, keys);
-            float n0, n1, n2, spare;
-            normals3_spare(w, n0, n1, n2, spare);
+            float n0, n1, n2;
+            normals3(w, s_ntab, n0, n1, n2);
             bool acc_e, mv_e;
             int ce_old, ce_new;
             {
@@ -1106,7 +1102,7 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
             rx = last ? xo : rx;
             ry = last ? yo : ry;
             rz = last ? zo : rz;
-            normals3_odd(spare, wo, n0, n1, n2);
+            normals3(wo, s_ntab, n0, n1, n2);
             bool acc_o, mv_o;
             int co_old, co_new;
             {
@@ -1603,8 +1599,7 @@ __global__ void k_unpack16(const SysDev* S, uint32_t* out, int64_t n) {
 }
 
 // ------------------------------------------------------------ diagnostics
-__global__ void k_debug_math(uint32_t k0, uint32_t k1, int n, uint32_t* words, float* logs, float* sines,
-                             float* cosines, float* normals) {
+__global__ void k_debug_math(uint32_t k0, uint32_t k1, int n, uint32_t* words, float* logs, float* normals) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint4 w = philox4x32_10(make_uint4((uint32_t)i, 0u, 0u, 0u), k0, k1);
@@ -1612,22 +1607,17 @@ __global__ void k_debug_math(uint32_t k0, uint32_t k1, int n, uint32_t* words, f
     words[4 * i + 1] = w.y;
     words[4 * i + 2] = w.z;
     words[4 * i + 3] = w.w;
-    logs[i] = log_f(u01(w.x));
-    float s, c;
-    sincos_turn(w.y, s, c);
-    sines[i] = s;
-    cosines[i] = c;
+    logs[i] = log_f(u01(w.w));
     float n0, n1, n2;
-    normals3(w, n0, n1, n2);
+    normals3(w, normal_table(), n0, n1, n2);
     normals[3 * i] = n0;
     normals[3 * i + 1] = n1;
     normals[3 * i + 2] = n2;
 }
 
 // -------------------------------------------------------------- launchers
-int launch_debug_math(uint32_t k0, uint32_t k1, int n, uint32_t* words, float* logs, float* sines, float* cosines,
-                      float* normals, void* stream) {
-    k_debug_math<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(k0, k1, n, words, logs, sines, cosines, normals);
+int launch_debug_math(uint32_t k0, uint32_t k1, int n, uint32_t* words, float* logs, float* normals, void* stream) {
+    k_debug_math<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(k0, k1, n, words, logs, normals);
     return (int)cudaGetLastError();
 }
 
@@ -1796,7 +1786,7 @@ static int launch_sweep_t(const MoveTile* tiles, int n_tiles, int mtb, int ml, L
         // per-warp slice: ceil(chains per tile / warps) chains of the longest length
         const int nw = sh.threads / 32;
         const int wb = ((sh.max_chains + nw - 1) / nw) * ml;
-        const size_t smem = (size_t)nw * (3 * wb + (wb + 1) / 2) * sizeof(float);
+        const size_t smem = (size_t)nw * 3 * wb * sizeof(float);
         if (smem > sweep_smem_bytes(kMaxTileBeads, kMaxLength)) return (int)cudaErrorInvalidValue;
         if (keys == kKeysBoth)
             k_sweep_linear<MODE, kKeysBoth><<<blocks, sh.threads, smem, st>>>(tiles, nullptr, n_tiles, wb, acc, sh.keys);

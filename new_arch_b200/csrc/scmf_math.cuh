@@ -1,5 +1,6 @@
 // Device arithmetic of the SCMF engine: counter-based Philox4x32-10, uniform
-// and Gaussian variates, and project-written log / sin / cos.
+// and Gaussian variates (a tabulated inverse normal CDF), and a project-written
+// log.
 //
 // Every routine is IEEE single precision built from +, -, *, correctly rounded
 // division and sqrt, and explicit __fmaf_rn; the translation unit is compiled
@@ -103,110 +104,36 @@ __device__ __forceinline__ float log_floor(float u) {
     return __fmaf_rn(__int2float_rn(e), 0x1.62e430p-1f, -0x1p-10f);
 }
 
-// -2 ln u for u in (0, 1]: the squared Box-Muller radius.  u = 2^k m with m in
-// [sqrt(1/2), sqrt(2)) split off in integers (k from the bits of u minus those
-// of sqrt(1/2)), t = m - 1 exact, -2 log1p(t) = -2t + t^2 Q2(t) with Q2 = -2 Q
-// of log_f (the same fit, scaled by -2 exactly), and -2 k ln2 added with
-// -2 ln2 rounded to FP32 (at most 9e-8 off for the k >= -23 that u01 yields).
-__device__ __forceinline__ float rad2_f(float u) {
-    const uint32_t ix = __float_as_uint(u) - 0x3F3504F3u;
-    const int k = (int)ix >> 23;
-    const float t = __fsub_rn(__uint_as_float((ix & 0x007FFFFFu) + 0x3F3504F3u), 1.0f);
-    float q = 0x1.321a4cp-3f;
-    q = __fmaf_rn(q, t, -0x1.068b2ap-2f);
-    q = __fmaf_rn(q, t, 0x1.0f9b0cp-2f);
-    q = __fmaf_rn(q, t, -0x1.22bf86p-2f);
-    q = __fmaf_rn(q, t, 0x1.5424e0p-2f);
-    q = __fmaf_rn(q, t, -0x1.999fc2p-2f);
-    q = __fmaf_rn(q, t, 0x1.000422p-1f);
-    q = __fmaf_rn(q, t, -0x1.555558p-1f);
-    q = __fmaf_rn(q, t, 0x1.fffff8p-1f);
-    const float r2 = __fmaf_rn(__fmul_rn(t, t), q, __fmul_rn(-2.0f, t));
-    return __fmaf_rn(__int2float_rn(k), -0x1.62e430p+0f, r2);
+// One standard normal from one 32-bit word by the inverse normal CDF: bit 31
+// is the sign, bits 0..30 give f = 2 (w mod 2^31) + 1 rounded to FP32 (in
+// [1, 2^32]) and the magnitude is the half-normal quantile h(f 2^-32),
+// h(v) = -Phi^-1(v / 2), from a table of 513 cubic segments (16 per binade
+// of f, picked by the exponent and the top four mantissa bits; the local
+// coordinate t in [-2^-5, 2^-5) is the low 19 mantissa bits, exactly).  The
+// table (scmf_normal_table.h, written by gen_normal_table.py) is within
+// 1.3e-7 relative of the quantile, and reaches 6.34 sigma.  `tab` points at a
+// copy of the table in shared memory in the move kernels, at the global one
+// elsewhere; the bits are the same.
+__device__ __forceinline__ float normal_of(uint32_t w, const float4* __restrict__ tab) {
+    const uint32_t b = __float_as_uint(__uint2float_rn((w << 1) | 1u));
+    const float4 c = tab[(b >> 19) - (127u << 4)];
+    const float t = __fsub_rn(__uint_as_float((b & 0x7FFFFu) | 0x3F800000u), 1.03125f);
+    float z = __fmaf_rn(c.w, t, c.z);
+    z = __fmaf_rn(z, t, c.y);
+    z = __fmaf_rn(z, t, c.x);
+    return __uint_as_float(__float_as_uint(z) ^ (w & 0x80000000u));
 }
 
-// sin and cos of 2 pi (2j+1) 2^-24 with j = w >> 9: the quadrant is removed in
-// integers, the remainder g in [-1/2, 1/2) of a quadrant goes through
-// sin(pi g / 2) = g S(g^2) (to g^7) and cos(pi g / 2) = 1 + g^2 C(g^2) (to g^8),
-// S and C fitted by least squares on Chebyshev nodes (gen_sincos_poly.py;
-// at most 1e-7 absolute error in FP32).
-__device__ __forceinline__ void sincos_turn(uint32_t w, float& s, float& c) {
-    const int32_t v = (int32_t)(((w >> 9) << 1) | 1u);
-    const int32_t qv = (v + (1 << 21)) >> 22;
-    const int32_t r = v - (qv << 22);
-    const int q = qv & 3;
-    const float g = __fmul_rn(__int2float_rn(r), 0x1p-22f);
-    const float g2 = __fmul_rn(g, g);
-    float sp = -0x1.2cf598p-8f;
-    sp = __fmaf_rn(sp, g2, 0x1.465a3cp-4f);
-    sp = __fmaf_rn(sp, g2, -0x1.4abba8p-1f);
-    sp = __fmaf_rn(sp, g2, 0x1.921fb4p+0f);
-    const float sa = __fmul_rn(g, sp);
-    float cp = 0x1.d9f188p-11f;
-    cp = __fmaf_rn(cp, g2, -0x1.55c64ap-6f);
-    cp = __fmaf_rn(cp, g2, 0x1.03c1dep-2f);
-    cp = __fmaf_rn(cp, g2, -0x1.3bd3ccp+0f);
-    const float ca = __fmaf_rn(cp, g2, 1.0f);
-    const bool odd = q & 1, neg_s = q & 2, neg_c = (q == 1) || (q == 2);
-    const float s0 = odd ? ca : sa;
-    const float c0 = odd ? sa : ca;
-    s = neg_s ? -s0 : s0;
-    c = neg_c ? -c0 : c0;
+// The three normals of a move from words x, y, z of its Philox block.
+__device__ __forceinline__ void normals3(uint4 w, const float4* __restrict__ tab, float& n0, float& n1, float& n2) {
+    n0 = normal_of(w.x, tab);
+    n1 = normal_of(w.y, tab);
+    n2 = normal_of(w.z, tab);
 }
 
-// Three standard normals from one Philox block (Box-Muller on (w.x, w.y) and
-// on (w.z, w.w), the last sine unused).  Only bits 8..31 of each word are
-// read; the low bytes feed accept_word().
-__device__ __forceinline__ void normals3(uint4 w, float& n0, float& n1, float& n2) {
-    float s, c;
-    const float r0 = __fsqrt_rn(rad2_f(u01(w.x)));
-    sincos_turn(w.y, s, c);
-    n0 = __fmul_rn(r0, c);
-    n1 = __fmul_rn(r0, s);
-    const float r1 = __fsqrt_rn(rad2_f(u01(w.z)));
-    sincos_turn(w.w, s, c);
-    n2 = __fmul_rn(r1, c);
-}
-
-// normals3 that also returns the spare sine of its second Box-Muller pair
-// (the first normal of the next, odd, bead).
-__device__ __forceinline__ void normals3_spare(uint4 w, float& n0, float& n1, float& n2, float& spare) {
-    float s, c;
-    const float r0 = __fsqrt_rn(rad2_f(u01(w.x)));
-    sincos_turn(w.y, s, c);
-    n0 = __fmul_rn(r0, c);
-    n1 = __fmul_rn(r0, s);
-    const float r1 = __fsqrt_rn(rad2_f(u01(w.z)));
-    sincos_turn(w.w, s, c);
-    n2 = __fmul_rn(r1, c);
-    spare = __fmul_rn(r1, s);
-}
-
-// The spare sine of bead b-1's block, for an odd bead b whose even partner is
-// not at hand.
-__device__ __forceinline__ float spare_of(uint4 wp) {
-    float s, c;
-    const float r1 = __fsqrt_rn(rad2_f(u01(wp.z)));
-    sincos_turn(wp.w, s, c);
-    return __fmul_rn(r1, s);
-}
-
-// Normals of an odd bead: the spare sine of bead b-1, then Box-Muller on
-// (w.x, w.y) of its own block.  Three Box-Muller pairs per two beads.
-__device__ __forceinline__ void normals3_odd(float spare, uint4 w, float& n0, float& n1, float& n2) {
-    float s, c;
-    const float r = __fsqrt_rn(rad2_f(u01(w.x)));
-    sincos_turn(w.y, s, c);
-    n0 = spare;
-    n1 = __fmul_rn(r, c);
-    n2 = __fmul_rn(r, s);
-}
-
-// The Metropolis uniform of a move: the low bytes of w.y, w.z, w.w of the
-// block that gave its normals (bits the normals never read).
-__device__ __forceinline__ uint32_t accept_word(uint4 w) {
-    return ((w.y & 0xFFu) << 24) | ((w.z & 0xFFu) << 16) | ((w.w & 0xFFu) << 8);
-}
+// The Metropolis word of a move: word w of the same block (u01 reads its bits
+// 9..31).
+__device__ __forceinline__ uint32_t accept_word(uint4 w) { return w.w; }
 
 // floor(x * inv_d) mod n, in [0, n), for |x * inv_d| < 2^22 (beyond that the
 // index stays in [0, n) but need not be the floor).  FP32 restatement of the

@@ -312,12 +312,10 @@ def _tune_dict(t: _lib.Tune) -> dict:
 
 
 def debug_math(n: int, key=(0, 0)):
-    """Device Philox words, log, sin, cos and normals for counters (i,0,0,0)."""
+    """Device Philox words, Metropolis log and normals for counters (i,0,0,0)."""
     words = np.zeros(4 * n, dtype=np.uint32)
     logs = np.zeros(n, dtype=np.float32)
-    s = np.zeros(n, dtype=np.float32)
-    c = np.zeros(n, dtype=np.float32)
     nr = np.zeros(3 * n, dtype=np.float32)
     check(lib().scmf_debug_math(key[0], key[1], n, _ptr(words, C.c_uint32), _ptr(logs, C.c_float),
-                                _ptr(s, C.c_float), _ptr(c, C.c_float), _ptr(nr, C.c_float)))
-    return words.reshape(-1, 4), logs, s, c, nr.reshape(-1, 3)
+                                _ptr(nr, C.c_float)))
+    return words.reshape(-1, 4), logs, nr.reshape(-1, 3)

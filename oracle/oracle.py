@@ -91,7 +91,8 @@ def lib():
     L.orc_logf.argtypes = [C.c_float]
     L.orc_log_floor_violations.restype = C.c_long
     L.orc_log_floor_violations.argtypes = [C.c_float, C.c_float, C.POINTER(C.c_float)]
-    L.orc_sincos_turn.argtypes = [C.c_uint32, f32p, f32p]
+    L.orc_normal.restype = C.c_float
+    L.orc_normal.argtypes = [C.c_uint32]
     L.orc_normals3.argtypes = [u32p, f32p, f32p, f32p]
     L.orc_u01.restype = C.c_float
     L.orc_u01.argtypes = [C.c_uint32]
@@ -126,10 +127,9 @@ def logf(x: float) -> float:
     return lib().orc_logf(C.c_float(x))
 
 
-def sincos_turn(w: int):
-    s, c = C.c_float(), C.c_float()
-    lib().orc_sincos_turn(C.c_uint32(w), C.byref(s), C.byref(c))
-    return s.value, c.value
+def normal(w: int) -> float:
+    """The standard normal of one 32-bit word (tabulated inverse CDF)."""
+    return lib().orc_normal(C.c_uint32(w))
 
 
 def normals3(w):

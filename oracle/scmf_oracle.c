@@ -14,9 +14,8 @@
  *   for every chain, for colour c = 0 .. n_colours-1, for every bead b of
  *   colour c: a smart-MC (force-biased, Rossky-Doll-Friedman) trial against the
  *   frozen omega field.  The Philox4x32-10 block with counter (chain, b, s, 0)
- *   gives the Gaussian displacement of bead b (an odd bead also takes the
- *   spare sine of bead b-1's block) and, from the bytes the normals do not
- *   read, its Metropolis uniform.
+ *   gives the Gaussian displacement of bead b (words 0..2, one normal each by
+ *   a tabulated inverse normal CDF) and its Metropolis uniform (word 3).
  *   Bonded beads never share a colour, so the result does not depend on the
  *   order in which beads of one colour are visited, nor on chain order.
  * The reference instead draws `length` random beads with replacement per chain
@@ -24,6 +23,7 @@
  * order and is applied identically here and on the GPU.
  */
 #include "scmf_oracle.h"
+#include "../new_arch_b200/csrc/scmf_normal_table.h"
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -107,91 +107,39 @@ float orc_logf(float x) {
     return fmaf(fe, 0x1.62ep-1f, fmaf(fe, 0x1.0bfbe8p-15f, lm));
 }
 
-/* -2 ln u for u in (0, 1], the squared Box-Muller radius: u = 2^k m with m in
- * [sqrt(1/2), sqrt(2)) from the bits of u minus those of sqrt(1/2), t = m - 1
- * (exact), -2 log1p(t) = -2t + t^2 Q2(t) with Q2 = -2 Q of orc_logf (scaled
- * exactly), plus k times -2 ln2 rounded to FP32. */
-float orc_rad2(float u) {
-    const uint32_t ix = f2u(u) - 0x3F3504F3u;
-    const int k = (int32_t)ix >> 23;
-    const float t = u2f((ix & 0x007FFFFFu) + 0x3F3504F3u) - 1.0f;
-    float q = 0x1.321a4cp-3f;
-    q = fmaf(q, t, -0x1.068b2ap-2f);
-    q = fmaf(q, t, 0x1.0f9b0cp-2f);
-    q = fmaf(q, t, -0x1.22bf86p-2f);
-    q = fmaf(q, t, 0x1.5424e0p-2f);
-    q = fmaf(q, t, -0x1.999fc2p-2f);
-    q = fmaf(q, t, 0x1.000422p-1f);
-    q = fmaf(q, t, -0x1.555558p-1f);
-    q = fmaf(q, t, 0x1.fffff8p-1f);
-    const float r2 = fmaf(t * t, q, -2.0f * t);
-    return fmaf((float)k, -0x1.62e430p+0f, r2);
+/* The inverse normal CDF table: 513 cubic segments (c0, c1, c2, c3) of the
+ * half-normal quantile h(v) = -Phi^-1(v / 2), written by
+ * new_arch_b200/csrc/gen_normal_table.py (data shared with the kernels;
+ * tests/test_oracle.py checks it against an independent quantile). */
+static const float orc_normal_tab[SCMF_NORMAL_SEGS * 4] = {SCMF_NORMAL_TABLE_DATA};
+
+/* One standard normal from one 32-bit word: bit 31 is the sign, bits 0..30
+ * give f = float(2 (w mod 2^31) + 1) (rounded to nearest) in [1, 2^32], and
+ * the magnitude is h(f 2^-32) from segment (bits(f) >> 19) - 127*16 (exponent
+ * and top four mantissa bits) at t = (1 + m19 2^-23) - (1 + 2^-5), m19 the
+ * low 19 mantissa bits (exact), by Horner with fmaf. */
+float orc_normal(uint32_t w) {
+    const uint32_t b = f2u((float)((w << 1) | 1u));
+    const float* c = orc_normal_tab + 4 * (size_t)((b >> 19) - (127u << 4));
+    const float t = u2f((b & 0x7FFFFu) | 0x3F800000u) - 1.03125f;
+    float z = fmaf(c[3], t, c[2]);
+    z = fmaf(z, t, c[1]);
+    z = fmaf(z, t, c[0]);
+    return u2f(f2u(z) ^ (w & 0x80000000u));
 }
 
-/* sin and cos of the angle 2*pi*(2j+1)*2^-24, j = w >> 9.  The quadrant is
- * split off in integers, the remainder g in [-1/2, 1/2) of a quadrant goes
- * through sin(pi g/2) = g S(g^2) (to g^7) and cos(pi g/2) = 1 + g^2 C(g^2) (to
- * g^8), the fits of new_arch_b200/csrc/gen_sincos_poly.py. */
-void orc_sincos_turn(uint32_t w, float* s, float* c) {
-    int32_t v = (int32_t)(((w >> 9) << 1) | 1u);
-    int32_t qv = (v + (1 << 21)) >> 22;
-    int32_t r = v - (qv << 22);
-    int q = qv & 3;
-    float g = (float)r * 0x1p-22f;
-    float g2 = g * g;
-    float sp = -0x1.2cf598p-8f;
-    sp = fmaf(sp, g2, 0x1.465a3cp-4f);
-    sp = fmaf(sp, g2, -0x1.4abba8p-1f);
-    sp = fmaf(sp, g2, 0x1.921fb4p+0f);
-    float sa = g * sp;
-    float cp = 0x1.d9f188p-11f;
-    cp = fmaf(cp, g2, -0x1.55c64ap-6f);
-    cp = fmaf(cp, g2, 0x1.03c1dep-2f);
-    cp = fmaf(cp, g2, -0x1.3bd3ccp+0f);
-    float ca = fmaf(cp, g2, 1.0f);
-    switch (q) {
-        case 0: *s = sa; *c = ca; break;
-        case 1: *s = ca; *c = -sa; break;
-        case 2: *s = -sa; *c = -ca; break;
-        default: *s = -ca; *c = sa; break;
-    }
-}
-
-/* Three standard normals from one Philox block: Box-Muller on (w0,w1) gives
- * n0 = r cos, n1 = r sin; on (w2,w3) gives n2 = r cos (the fourth is unused,
- * as curand_normal4's w is unused in device_function.cu:683-688).  Only bits
- * 8..31 of each word are read; the low bytes feed orc_accept_word(). */
+/* The three normals of a move: words 0, 1, 2 of its Philox block.  The
+ * reference draws them with curand_normal4 (device_function.cu:683-688), its
+ * fourth value unused; here the fourth word is the Metropolis word. */
 void orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2) {
-    float s, c;
-    float r0 = sqrtf(orc_rad2(orc_u01(w[0])));
-    orc_sincos_turn(w[1], &s, &c);
-    *n0 = r0 * c;
-    *n1 = r0 * s;
-    float r1 = sqrtf(orc_rad2(orc_u01(w[2])));
-    orc_sincos_turn(w[3], &s, &c);
-    *n2 = r1 * c;
+    *n0 = orc_normal(w[0]);
+    *n1 = orc_normal(w[1]);
+    *n2 = orc_normal(w[2]);
 }
 
-/* Normals of an odd bead b: the first is the sine partner of bead b-1's third
- * normal (the unused half of Box-Muller on (wp[2], wp[3]), wp = block of b-1);
- * the other two are Box-Muller on (w[0], w[1]) of its own block.  Three
- * Box-Muller pairs per two beads. */
-void orc_normals3_odd(const uint32_t wp[4], const uint32_t w[4], float* n0, float* n1, float* n2) {
-    float s, c;
-    float rb = sqrtf(orc_rad2(orc_u01(wp[2])));
-    orc_sincos_turn(wp[3], &s, &c);
-    *n0 = rb * s;
-    float r = sqrtf(orc_rad2(orc_u01(w[0])));
-    orc_sincos_turn(w[1], &s, &c);
-    *n1 = r * c;
-    *n2 = r * s;
-}
-
-/* The Metropolis uniform of a move comes from the same Philox block: the low
- * bytes of w1, w2, w3, which the normals never read. */
-uint32_t orc_accept_word(const uint32_t w[4]) {
-    return ((w[1] & 0xFFu) << 24) | ((w[2] & 0xFFu) << 16) | ((w[3] & 0xFFu) << 8);
-}
+/* The Metropolis word of a move: word 3 of the same block (orc_u01 reads its
+ * bits 9..31). */
+uint32_t orc_accept_word(const uint32_t w[4]) { return w[3]; }
 
 /* Periodic fold of one coordinate to a cell index in [0, n): floor(x/dx) mod n
  * (for |x/dx| < 2^22, the range the kernels support).  Restates
@@ -553,21 +501,14 @@ float orc_trial_energy(const orc_system* s, int arch, int b, const float* X, con
     return trial_energy(s, a, b, X, Y, Z, n0, n1, n2, p_out, p_out + 1, p_out + 2);
 }
 
-/* One trial of bead b: its Philox block (chain, b, step, 0) gives the
- * Metropolis word and the normals (even b: normals3; odd b: see
- * orc_normals3_odd, which also reads the block of bead b-1). */
+/* One trial of bead b: its Philox block (chain, b, step, 0) gives the three
+ * normals and the Metropolis word. */
 static inline int move_single(const orc_system* s, const orc_arch* a, uint32_t gc, int b,
                               float* X, float* Y, float* Z, const uint32_t key[2], uint32_t step) {
     uint32_t ctr[4] = {gc, (uint32_t)b, step, 0u}, w[4];
     orc_philox4x32_10(ctr, key, w);
     float n0, n1, n2;
-    if (b & 1) {
-        uint32_t cp[4] = {gc, (uint32_t)(b - 1), step, 0u}, wp[4];
-        orc_philox4x32_10(cp, key, wp);
-        orc_normals3_odd(wp, w, &n0, &n1, &n2);
-    } else {
-        orc_normals3(w, &n0, &n1, &n2);
-    }
+    orc_normals3(w, &n0, &n1, &n2);
     return move_bead(s, a, b, X, Y, Z, n0, n1, n2, orc_accept_word(w));
 }
 

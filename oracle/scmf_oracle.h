@@ -92,10 +92,8 @@ int  orc_analyze(const orc_system* s, int arch, double* out);
 void  orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 float orc_logf(float x);
 long orc_log_floor_violations(float ln2_f, float slack, float* min_margin);
-void  orc_sincos_turn(uint32_t w, float* s, float* c);
-float orc_rad2(float u);   /* -2 ln u, the squared Box-Muller radius */
+float orc_normal(uint32_t w);   /* one standard normal from one word (inverse CDF) */
 void  orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2);
-void  orc_normals3_odd(const uint32_t wp[4], const uint32_t w[4], float* n0, float* n1, float* n2);
 float orc_u01(uint32_t w);
 uint32_t orc_accept_word(const uint32_t w[4]);
 int   orc_fold(float x, float inv_d, int n);

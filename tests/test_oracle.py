@@ -40,38 +40,40 @@ def test_log_accuracy():
     assert max(abs(orc.logf(float(x)) - math.log(float(x))) for x in near) < 2e-8
 
 
-def test_box_muller_radius_accuracy():
-    """The squared Box-Muller radius -2 ln u against FP64 for a spread of the
-    2^23 uniforms u01 yields (all exponents, both ends): within 3e-7 relative,
-    and within 4e-8 absolute near u = 1 where it goes to zero."""
-    import ctypes as C
-    L = orc.lib()
-    L.orc_rad2.restype = C.c_float
-    L.orc_rad2.argtypes = [C.c_float]
+def _normal_words():
+    """Random words, the two ends of the magnitude (f = 1 and f near 2^32), and
+    words at and just below every segment boundary of the table, both signs."""
     rng = np.random.default_rng(4)
-    words = np.concatenate([rng.integers(0, 2 ** 32, 30000, dtype=np.uint64),
-                            np.arange(0, 4096, dtype=np.uint64) << np.uint64(9),
-                            (np.uint64(2 ** 23 - 1) - np.arange(0, 4096, dtype=np.uint64)) << np.uint64(9)])
-    worst_rel = worst_abs = 0.0
-    for w in words:
-        u = L.orc_u01(int(w))
-        want = -2.0 * math.log(u)
-        got = L.orc_rad2(u)
-        if want > 1e-3:
-            worst_rel = max(worst_rel, abs(got - want) / want)
-        else:
-            worst_abs = max(worst_abs, abs(got - want))
-    assert worst_rel < 3e-7 and worst_abs < 4e-8, (worst_rel, worst_abs)
+    words = [rng.integers(0, 2 ** 32, 60000, dtype=np.uint64),
+             np.arange(0, 2048, dtype=np.uint64), np.uint64(0x7FFFFFFF) - np.arange(0, 2048, dtype=np.uint64)]
+    for e in range(32):
+        for j in range(16):
+            f = (2 ** e) * (16 + j) // 16          # segment start (integer part), its odd neighbours
+            for d in (-3, -1, 1, 3):
+                v = f + d
+                if 1 <= v < 2 ** 32 and v % 2 == 1:
+                    words.append(np.array([(v - 1) // 2], dtype=np.uint64))
+    w = np.concatenate(words)
+    return np.concatenate([w, w | np.uint64(0x80000000)])
 
 
-def test_sincos_accuracy():
-    rng = np.random.default_rng(2)
-    worst = 0.0
-    for w in rng.integers(0, 2 ** 32, 20000, dtype=np.uint64):
-        s, c = orc.sincos_turn(int(w))
-        th = 2 * math.pi * (((int(w) >> 9) << 1) | 1) * 2.0 ** -24
-        worst = max(worst, abs(s - math.sin(th)), abs(c - math.cos(th)))
-    assert worst < 1.5e-7
+def test_normal_quantile_accuracy():
+    """The normal of a word against an independent quantile (scipy's ndtri in
+    FP64) of the same rounded variate: v = float32(2 (w mod 2^31) + 1) 2^-32,
+    z = sign * -ndtri(v / 2).  Within 1.5e-7 relative above |z| = 0.5, within
+    7.5e-8 absolute below; the tail reaches 6.3 sigma."""
+    from scipy.special import ndtri
+    words = _normal_words()
+    f = ((words & np.uint64(0x7FFFFFFF)) * np.uint64(2) + np.uint64(1)).astype(np.float64).astype(np.float32)
+    v = f.astype(np.float64) * 2.0 ** -32
+    sign = np.where(words & np.uint64(0x80000000), -1.0, 1.0)
+    want = sign * -ndtri(v / 2.0)
+    got = np.array([orc.normal(int(w)) for w in words], dtype=np.float64)
+    err = np.abs(got - want)
+    big = np.abs(want) > 0.5
+    assert (err[big] / np.abs(want[big])).max() < 1.5e-7
+    assert err[~big].max() < 7.5e-8
+    assert np.abs(want).max() > 6.3 and np.abs(got).max() > 6.3
 
 
 def test_uniform_range():
