@@ -501,6 +501,21 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
             c.cdeg[g] = h.cdeg[g];
             c.ac4deg[g] = h.ac4deg[g];
         }
+        c.sys = d_sys;
+        c.n_arch = 0;
+        for (size_t a = 0; a < archs.size(); ++a) {
+            if (archs[a].n_chains == 0) continue;
+            if (c.n_arch == kLeanMaxArch) {
+                p->lean_ok = false;
+                break;
+            }
+            LeanArch& la = c.arch[c.n_arch++];
+            la.types = h_arch[a].types;
+            la.length = archs[a].length;
+            la.n_chains = archs[a].n_chains;
+            la.chain0 = archs[a].chain_base;
+            la.bead0 = (int32_t)archs[a].bead_base;
+        }
     } else {
         if (p->seed != spec.p.seed) p->one_seed = false;
         if ((p->seed >> 32) != (spec.p.seed >> 32)) p->one_seed_hi = false;

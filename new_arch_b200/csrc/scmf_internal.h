@@ -181,6 +181,17 @@ enum KeyMode { kKeysNone = 0, kKeysHigh = 1, kKeysBoth = 2 };
 // single-system move kernel reads them from the parameter constant bank
 // (instruction operands) instead of loading them from SysDev into registers.
 // Fixed for the life of the system: device buffers and spec constants.
+// One architecture of the system the lean move kernel moves: linear chains of
+// an even length with length / 2 dividing 32.
+struct LeanArch {
+    const uint8_t* types;  // [length], monomer type per bead
+    int32_t length;
+    int32_t n_chains;
+    int32_t chain0;        // first chain (index into chain_id)
+    int32_t bead0;         // first bead
+};
+constexpr int kLeanMaxArch = 4;
+
 struct SysConsts {
     float* x;
     float* y;
@@ -191,6 +202,9 @@ struct SysConsts {
     float k2, A, R, inv_dx, inv_dy, inv_dz;
     int32_t nx, ny, nz, pad;
     float cdeg[3], ac4deg[3];  // c = 2k deg and A c / 4 for 0, 1, 2 bonds
+    SysDev* sys;
+    int32_t n_arch, pad2;
+    LeanArch arch[kLeanMaxArch];
 };
 
 struct LaunchShape {

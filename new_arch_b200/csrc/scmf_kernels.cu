@@ -805,21 +805,31 @@ __global__ void __maxnreg__(reg_cap(ANY_FLAT, FOLD, KEYS)) k_sweep_reg(const Mov
 // such launches).  Same sweep, trials and random numbers as k_sweep_reg, with
 // less work per trial:
 //  * the system's constants (positions, omega, chain ids, k, A, R, cell
-//    inverses, grid, per-degree c and A c / 4) come from the parameter bank
-//    (SysConsts), the Philox round keys too;
+//    inverses, grid, per-degree c and A c / 4, the architectures' chain and
+//    bead ranges) come from the parameter bank (SysConsts), the Philox round
+//    keys too;
 //  * every pair has an odd bead, so the even/odd branches go away; a missing
 //    bond neighbour at a chain end is replaced by the bead itself, whose term
 //    fma(+0, 2k, f) leaves the force bit for bit as if it were skipped (the
 //    force starts at +0 and can only be -0 from a -0 sum, which RN never
 //    gives here);
-//  * lanes beyond the tile's last chain (a partial last iteration) repeat the
-//    last chain and store nothing, so every lane runs the same code;
+//  * lanes beyond an architecture's last chain (a partial last group) repeat
+//    that chain and store nothing, so every lane runs the same code;
 //  * the Metropolis logarithm and the count moves sit under warp-uniform
 //    branches (__any_sync); the outcome of every trial is unchanged.
-// Bead and cell indices are 32-bit (the plan checks the sizes).  Each warp
-// loads the next iteration's pairs while it moves the current ones; at 72
-// registers (seven 128-thread CTAs per SM) that took the large system's move
-// launch from 0.511 to 0.496 ms (0.513 ms at 64 registers without it).
+// Persistent: one CTA of kLeanThreads (28 warps, 72 registers each: the SM's
+// whole register file) per SM.  Each warp strides over the groups of 32/(L/2)
+// chains of every architecture, so no tile tail is left, and loads the next
+// group's pairs while it moves the current one.  The CTA keeps kLeanCopies
+// copies of the normal table in shared memory, entry-interleaved, and lane l
+// reads copy l % 8: the eight lanes of one 16-byte shared-memory phase then
+// always read eight different bank groups (with one copy, random segments made
+// 2.3 wavefronts of every phase).  Bead and cell indices are 32-bit (the plan
+// checks the sizes).
+constexpr int kLeanThreads = 896;
+constexpr int kLeanCopies = 8;
+constexpr size_t kLeanSmem = (size_t)SCMF_NORMAL_SEGS * kLeanCopies * sizeof(float4);
+
 __device__ __forceinline__ bool trial_lean(const MoveConsts& c, float x, float y, float z, float fx, float fy,
                                            float fz, float cc, float ac4, float n0, float n1, float n2, uint32_t aw,
                                            const float* __restrict__ w_t, float& px, float& py, float& pz,
@@ -847,11 +857,18 @@ __device__ __forceinline__ bool trial_lean(const MoveConsts& c, float x, float y
 }
 
 template <int MODE>
-__global__ void __maxnreg__(72) k_sweep_lean(const MoveTile* __restrict__ tiles, int n_tiles,
-                                             const PhiloxKeys keys, const SysConsts sc) {
-    __shared__ float4 s_ntab[SCMF_NORMAL_SEGS];
-    load_normal_table(s_ntab);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+__global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysConsts sc) {
+    extern __shared__ float4 s_ntab_lean[];  // [SCMF_NORMAL_SEGS][kLeanCopies]
+    for (int i = threadIdx.x; i < SCMF_NORMAL_SEGS * kLeanCopies; i += blockDim.x)
+        s_ntab_lean[i] = __ldg(normal_table() + i / kLeanCopies);
+    __syncthreads();
+    SysDev* S = sc.sys;
+    if (S->step >= S->stop_step) return;  // grid-uniform
+    const uint32_t step = S->step + 1u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gw = blockIdx.x * (blockDim.x >> 5) + warp;  // this warp among all
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    const float4* tab = s_ntab_lean + (lane & (kLeanCopies - 1));
     MoveConsts c;
     c.k = 0.0f;
     c.k2 = sc.k2;
@@ -865,46 +882,43 @@ __global__ void __maxnreg__(72) k_sweep_lean(const MoveTile* __restrict__ tiles,
     c.nz = sc.nz;
     c.pow2 = true;
     c.small = false;
-    for (int ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
-        const MoveTile t = tiles[ti];
-        SysDev* S = t.sys;
-        if (S->step >= S->stop_step) continue;  // block-uniform
-        const uint32_t step = S->step + 1u;
-        const ArchDev* Ap = t.arch;
-        const int L = Ap->length;
-        const int tpc = L >> 1;                                   // threads per chain, divides 32
-        const int cs = (int)div_magic((uint32_t)lane, Ap->tpc_magic, tpc);
-        const int tt = lane - cs * tpc;                           // pair index in the chain
-        const int cpw = 32 / tpc;                                 // chains per warp iteration
+    unsigned nacc = 0;
+    for (int a = 0; a < sc.n_arch; ++a) {
+        const int L = sc.arch[a].length;
+        const int lg = __ffs(L >> 1) - 1;                         // log2(L/2): L/2 divides 32
+        const int tpc = 1 << lg;                                  // threads per chain
+        const int cs = lane >> lg;                                // chain slot in the warp
+        const int tt = lane & (tpc - 1);                          // pair index in the chain
+        const int cpw = 32 >> lg;                                 // chains per group
         const int be = 2 * tt, bo = be + 1;
         const bool first = tt == 0, last = tt == tpc - 1;         // chain ends: one bond
         const float cc_e = first ? sc.cdeg[1] : sc.cdeg[2], ac4_e = first ? sc.ac4deg[1] : sc.ac4deg[2];
         const float cc_o = last ? sc.cdeg[1] : sc.cdeg[2], ac4_o = last ? sc.ac4deg[1] : sc.ac4deg[2];
-        const int toff_e = (int)__ldg(Ap->types + be) * (int)sc.n_cells;
-        const int toff_o = (int)__ldg(Ap->types + bo) * (int)sc.n_cells;
-        const int nch = t.n_chains;
-        const int stride = nwarps * cpw;
-        unsigned nacc = 0;
-        // the pair and chain id of the next iteration are loaded one iteration
-        // ahead, so the DRAM latency overlaps this iteration's trials
+        const int toff_e = (int)__ldg(sc.arch[a].types + be) * (int)sc.n_cells;
+        const int toff_o = (int)__ldg(sc.arch[a].types + bo) * (int)sc.n_cells;
+        const int nch = sc.arch[a].n_chains;
+        const int bead0 = sc.arch[a].bead0, chain0 = sc.arch[a].chain0;
+        const int groups = (nch + cpw - 1) >> (5 - lg);
+        // the pairs and chain id of the warp's next group are loaded one group
+        // ahead, so the DRAM latency overlaps this group's trials
         float2 nvx = make_float2(0.0f, 0.0f), nvy = nvx, nvz = nvx;
         uint32_t ngc = 0u;
-        auto fetch = [&](int cb) {
-            const int ch = min(cb + cs, nch - 1);
-            const int gn = (int)t.bead0 + ch * L + be;
+        auto fetch = [&](int grp) {
+            const int ch = min(grp * cpw + cs, nch - 1);
+            const int gn = bead0 + ch * L + be;
             nvx = __ldcs(reinterpret_cast<const float2*>(sc.x + gn));
             nvy = __ldcs(reinterpret_cast<const float2*>(sc.y + gn));
             nvz = __ldcs(reinterpret_cast<const float2*>(sc.z + gn));
-            ngc = __ldg(sc.chain_id + t.chain0 + ch);
+            ngc = __ldg(sc.chain_id + chain0 + ch);
         };
-        if (warp * cpw < nch) fetch(warp * cpw);
-        for (int cbase = warp * cpw; cbase < nch; cbase += stride) {  // warp-uniform bounds
-            const int chain = cbase + cs;
+        if (gw < groups) fetch(gw);
+        for (int grp = gw; grp < groups; grp += nw) {  // warp-uniform bounds
+            const int chain = grp * cpw + cs;
             const bool live = chain < nch;
-            const int g = (int)t.bead0 + (live ? chain : nch - 1) * L + be;
+            const int g = bead0 + (live ? chain : nch - 1) * L + be;
             const float2 vx = nvx, vy = nvy, vz = nvz;
             const uint32_t gc = ngc;
-            if (cbase + stride < nch) fetch(cbase + stride);
+            if (grp + nw < groups) fetch(grp + nw);
             float xe = vx.x, xo = vx.y, ye = vy.x, yo = vy.y, ze = vz.x, zo = vz.y;
             // even bead 2t: bonds to 2t-1 (lane - 1's odd bead; the bead itself at the chain start) and 2t+1
             float lx = __shfl_up_sync(0xffffffffu, xo, 1);
@@ -916,7 +930,7 @@ __global__ void __maxnreg__(72) k_sweep_lean(const MoveTile* __restrict__ tiles,
             const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), keys);
             const uint4 wo = philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys);
             float n0, n1, n2;
-            normals3(w, s_ntab, n0, n1, n2);
+            normals3<kLeanCopies>(w, tab, n0, n1, n2);
             bool acc_e, mv_e;
             int ce_old, ce_new;
             {
@@ -940,7 +954,7 @@ __global__ void __maxnreg__(72) k_sweep_lean(const MoveTile* __restrict__ tiles,
             rx = last ? xo : rx;
             ry = last ? yo : ry;
             rz = last ? zo : rz;
-            normals3(wo, s_ntab, n0, n1, n2);
+            normals3<kLeanCopies>(wo, tab, n0, n1, n2);
             bool acc_o, mv_o;
             int co_old, co_new;
             {
@@ -970,9 +984,9 @@ __global__ void __maxnreg__(72) k_sweep_lean(const MoveTile* __restrict__ tiles,
                 __stcs(reinterpret_cast<float2*>(sc.z + g), make_float2(ze, zo));
             }
         }
-        nacc = warp_sum(nacc);
-        if (lane == 0 && nacc) atomicAdd(&S->slot_acc[(ti * kMaxWarps + warp) % kSlots], (unsigned long long)nacc);
     }
+    nacc = warp_sum(nacc);
+    if (lane == 0 && nacc) atomicAdd(&S->slot_acc[gw % kSlots], (unsigned long long)nacc);
 }
 
 // The lean kernel's structure for launches of many systems (batches, served
@@ -1704,6 +1718,10 @@ int configure_kernels() {
     }
     cudaError_t ef = cudaMemcpyToSymbol(c_fold, fold_tab, sizeof fold_tab);
     if (ef != cudaSuccess) return (int)ef;
+    ef = cudaFuncSetAttribute(k_sweep_lean<kMoveOnly>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLeanSmem);
+    if (ef == cudaSuccess)
+        ef = cudaFuncSetAttribute(k_sweep_lean<kMoveGrid>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLeanSmem);
+    if (ef != cudaSuccess) return (int)ef;
     const int bytes = (int)sweep_smem_bytes(kMaxTileBeads, kMaxLength);
     cudaError_t e = cudaSuccess;
     for (int keys = kKeysNone; keys <= kKeysBoth && e == cudaSuccess; ++keys) {
@@ -1729,7 +1747,7 @@ static void launch_reg(const LaunchShape& sh, int blocks, int threads, cudaStrea
     const int keys = MODE == kGridOnly ? kKeysNone : sh.keyed;
     if constexpr (MODE != kGridOnly && !FLAT) {
         if (sh.lean && keys == kKeysBoth && sh.fold == 0 && !list) {
-            k_sweep_lean<MODE><<<blocks, threads, 0, st>>>(tiles, n, sh.keys, sh.sc);
+            k_sweep_lean<MODE><<<sm_count(), kLeanThreads, kLeanSmem, st>>>(sh.keys, sh.sc);
             return;
         }
         if (sh.warp_even) {

@@ -111,12 +111,13 @@ __device__ __forceinline__ float log_floor(float u) {
 // of f, picked by the exponent and the top four mantissa bits; the local
 // coordinate t in [-2^-5, 2^-5) is the low 19 mantissa bits, exactly).  The
 // table (scmf_normal_table.h, written by gen_normal_table.py) is within
-// 1.3e-7 relative of the quantile, and reaches 6.34 sigma.  `tab` points at a
-// copy of the table in shared memory in the move kernels, at the global one
-// elsewhere; the bits are the same.
+// 1.3e-7 relative of the quantile, and reaches 6.34 sigma.  `tab` points at
+// the global table, or at a lane's copy in shared memory where STRIDE copies
+// are entry-interleaved; the bits are the same.
+template <int STRIDE = 1>
 __device__ __forceinline__ float normal_of(uint32_t w, const float4* __restrict__ tab) {
     const uint32_t b = __float_as_uint(__uint2float_rn((w << 1) | 1u));
-    const float4 c = tab[(b >> 19) - (127u << 4)];
+    const float4 c = tab[((b >> 19) - (127u << 4)) * STRIDE];
     const float t = __fsub_rn(__uint_as_float((b & 0x7FFFFu) | 0x3F800000u), 1.03125f);
     float z = __fmaf_rn(c.w, t, c.z);
     z = __fmaf_rn(z, t, c.y);
@@ -125,10 +126,11 @@ __device__ __forceinline__ float normal_of(uint32_t w, const float4* __restrict_
 }
 
 // The three normals of a move from words x, y, z of its Philox block.
+template <int STRIDE = 1>
 __device__ __forceinline__ void normals3(uint4 w, const float4* __restrict__ tab, float& n0, float& n1, float& n2) {
-    n0 = normal_of(w.x, tab);
-    n1 = normal_of(w.y, tab);
-    n2 = normal_of(w.z, tab);
+    n0 = normal_of<STRIDE>(w.x, tab);
+    n1 = normal_of<STRIDE>(w.y, tab);
+    n2 = normal_of<STRIDE>(w.z, tab);
 }
 
 // The Metropolis word of a move: word w of the same block (u01 reads its bits
