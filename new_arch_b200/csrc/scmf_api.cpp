@@ -679,6 +679,11 @@ scmf_status scmf_set_omega(scmf_system* s, const float* in, size_t n) {
     const size_t want = (size_t)s->n_cells * s->spec.n_types;
     if (n != want) return fail(SCMF_E_INVALID, "expected %zu values, got %zu", want, n);
     CK(cudaMemcpyAsync(s->omega, in, want * 4, cudaMemcpyHostToDevice, s->stream));
+    // the caller's omega has no known span: the move kernels read every trial's
+    // omega until the next field step computes one
+    const float no_span = INFINITY;
+    CK(cudaMemcpyAsync((char*)s->d_sys + offsetof(SysDev, omega_span), &no_span, sizeof no_span,
+                       cudaMemcpyHostToDevice, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     return SCMF_OK;
 }

@@ -239,6 +239,9 @@ int fold_kind_of(const scmf_spec& s) {
 
 void fill_sysdev_constants(const scmf_spec& s, int64_t n_beads, SysDev* d) {
     d->stop_step = 0xFFFFFFFFu;
+    d->om_max_key = 0u;            // identities of the running max / min
+    d->om_min_key = 0xFFFFFFFFu;
+    d->omega_span = INFINITY;      // no bound until a field step computes one
     d->n_types = s.n_types;
     d->nx = s.nx; d->ny = s.ny; d->nz = s.nz;
     d->n_cells = (int64_t)s.nx * s.ny * s.nz;

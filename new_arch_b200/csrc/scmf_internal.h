@@ -102,6 +102,16 @@ struct SysDev {
     // counts the field step reads: NULL means counts[cur] (the grid of this
     // system's own beads); a chain shard points it at the sum over all shards
     const uint32_t* field_counts;
+    // the span of omega: every field step folds the largest and smallest
+    // non-NaN omega of its cells into om_max_key / om_min_key (order-preserving
+    // integer keys, reset by the block that closes the step) and publishes
+    // omega_span = max - min, so that omega_t[a] - omega_t[b] >= -omega_span for
+    // any two cells of a type.  The move kernels use it to reject trials
+    // without reading omega; +inf (after creation, scmf_set_omega or a
+    // checkpoint read) disables that until the next field step.
+    uint32_t om_max_key, om_min_key;
+    float omega_span;
+    uint32_t pad3;
     // the statistics of the last sweep in the public layout, written by
     // k_stats_out for asynchronous reads (scmf_step_stats_async)
     scmf_stats stats_out;

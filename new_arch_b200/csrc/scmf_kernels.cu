@@ -816,7 +816,10 @@ __global__ void __maxnreg__(reg_cap(ANY_FLAT, FOLD, KEYS)) k_sweep_reg(const Mov
 //  * lanes beyond an architecture's last chain (a partial last group) repeat
 //    that chain and store nothing, so every lane runs the same code;
 //  * the Metropolis logarithm and the count moves sit under warp-uniform
-//    branches (__any_sync); the outcome of every trial is unchanged.
+//    branches (__any_sync); the outcome of every trial is unchanged;
+//  * a trial whose bonded energy change alone exceeds what the omega span
+//    and its uniform allow is rejected before the cell folds and the omega
+//    gathers (maybe_accepted), which about half of the warps then skip.
 // Persistent: one CTA of kLeanThreads (28 warps, 72 registers each: the SM's
 // whole register file) per SM.  Each warp strides over the groups of 32/(L/2)
 // chains of every architecture, so no tile tail is left, and loads the next
@@ -830,10 +833,23 @@ constexpr int kLeanThreads = 896;
 constexpr int kLeanCopies = 8;
 constexpr size_t kLeanSmem = (size_t)SCMF_NORMAL_SEGS * kLeanCopies * sizeof(float4);
 
+// Rejection before the omega reads.  Every field step publishes span >= the
+// largest omega_t[a] - omega_t[b] (SysDev::omega_span), so, rounding being
+// monotone, fl(w_new - w_old) >= -span and dE = fl(fl(w_new - w_old) + deb) >=
+// fl(deb - span) =: lb.  A trial with -lb <= log_floor(u) <= log_f(u) has
+// dE > 0 and log_f(u) >= -dE: the Metropolis test below rejects it whatever
+// omega holds (and a NaN bound or energy rejects, as the test does).  At the
+// benchmark acceptance (~0.5 %) about 2 % of trials pass this bound, so about
+// half of the warps skip the cell folds, the two gathers and their L2 round
+// trip altogether; the outcome of every trial is the oracle's.
+__device__ __forceinline__ bool maybe_accepted(float deb, float span, float lf) {
+    return -__fsub_rn(deb, span) > lf;
+}
+
 __device__ __forceinline__ bool trial_lean(const MoveConsts& c, float x, float y, float z, float fx, float fy,
                                            float fz, float cc, float ac4, float n0, float n1, float n2, uint32_t aw,
-                                           const float* __restrict__ w_t, float& px, float& py, float& pz,
-                                           int& cell_old, int& cell_new) {
+                                           float span, const float* __restrict__ w_t, float& px, float& py,
+                                           float& pz, int& cell_old, int& cell_new) {
     const float A = c.A, R = c.R;
     const float dx = __fmaf_rn(A, fx, __fmul_rn(R, n0));
     const float dy = __fmaf_rn(A, fy, __fmul_rn(R, n1));
@@ -844,15 +860,20 @@ __device__ __forceinline__ bool trial_lean(const MoveConsts& c, float x, float y
     const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
     const float fd = __fmaf_rn(fx, dx, __fmaf_rn(fy, dy, __fmul_rn(fz, dz)));
     const float deb = __fmul_rn(ac4, __fmaf_rn(cc, d2, __fmul_rn(-2.0f, fd)));
-    cell_old = cell_of<0>(c, x, y, z);
-    cell_new = cell_of<0>(c, px, py, pz);
-    const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + cell_new), __ldg(w_t + cell_old)), deb);
-    // accept if dE < 0; else if dE < 17 and log(u) < -dE (log_floor decides
-    // without the logarithm for all but ~1 % of trials; see trial_f)
-    bool acc = dE < 0.0f;
     const float u = u01(aw);
-    const bool near = !acc && dE < 17.0f && -dE > log_floor(u);
-    if (__any_sync(0xffffffffu, near)) acc = acc || (near && log_f(u) < -dE);
+    bool acc = false;
+    cell_old = cell_new = 0;
+    if (__any_sync(0xffffffffu, maybe_accepted(deb, span, log_floor(u)))) {
+        cell_old = cell_of<0>(c, x, y, z);
+        cell_new = cell_of<0>(c, px, py, pz);
+        const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + cell_new), __ldg(w_t + cell_old)), deb);
+        // accept if dE < 0; else if log(u) < -dE (log_floor decides without the
+        // logarithm for all but ~1 % of trials; see trial_f; dE >= 17 fails
+        // -dE > log_floor(u) >= -23 ln2 - 2^-10)
+        acc = dE < 0.0f;
+        const bool near = !acc && -dE > log_floor(u);
+        if (__any_sync(0xffffffffu, near)) acc = acc || (near && log_f(u) < -dE);
+    }
     return acc;
 }
 
@@ -865,6 +886,7 @@ __global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysCon
     SysDev* S = sc.sys;
     if (S->step >= S->stop_step) return;  // grid-uniform
     const uint32_t step = S->step + 1u;
+    const float span = S->omega_span;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gw = blockIdx.x * (blockDim.x >> 5) + warp;  // this warp among all
     const int nw = gridDim.x * (blockDim.x >> 5);
@@ -939,8 +961,8 @@ __global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysCon
                 float fz = __fmaf_rn(__fsub_rn(lz, ze), c.k2, 0.0f);
                 add_bond(c.k2, xe, ye, ze, xo, yo, zo, fx, fy, fz);
                 float px, py, pz;
-                acc_e = trial_lean(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), sc.omega + toff_e,
-                                   px, py, pz, ce_old, ce_new) &&
+                acc_e = trial_lean(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), span,
+                                   sc.omega + toff_e, px, py, pz, ce_old, ce_new) &&
                         live;
                 xe = acc_e ? px : xe;
                 ye = acc_e ? py : ye;
@@ -963,8 +985,8 @@ __global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysCon
                 float fz = __fmaf_rn(__fsub_rn(ze, zo), c.k2, 0.0f);
                 add_bond(c.k2, xo, yo, zo, rx, ry, rz, fx, fy, fz);
                 float px, py, pz;
-                acc_o = trial_lean(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), sc.omega + toff_o,
-                                   px, py, pz, co_old, co_new) &&
+                acc_o = trial_lean(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), span,
+                                   sc.omega + toff_o, px, py, pz, co_old, co_new) &&
                         live;
                 xo = acc_o ? px : xo;
                 yo = acc_o ? py : yo;
@@ -999,8 +1021,8 @@ __global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysCon
 template <int FOLD>
 __device__ __forceinline__ bool trial_leanm(const MoveConsts& c, float x, float y, float z, float fx, float fy,
                                            float fz, float cc, float ac4, float n0, float n1, float n2, uint32_t aw,
-                                           const float* __restrict__ w_t, float& px, float& py, float& pz,
-                                           int& cell_old, int& cell_new) {
+                                           float span, const float* __restrict__ w_t, float& px, float& py,
+                                           float& pz, int& cell_old, int& cell_new) {
     const float A = c.A, R = c.R;
     const float dx = __fmaf_rn(A, fx, __fmul_rn(R, n0));
     const float dy = __fmaf_rn(A, fy, __fmul_rn(R, n1));
@@ -1011,15 +1033,18 @@ __device__ __forceinline__ bool trial_leanm(const MoveConsts& c, float x, float 
     const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
     const float fd = __fmaf_rn(fx, dx, __fmaf_rn(fy, dy, __fmul_rn(fz, dz)));
     const float deb = __fmul_rn(ac4, __fmaf_rn(cc, d2, __fmul_rn(-2.0f, fd)));
-    cell_old = cell_of<FOLD>(c, x, y, z);
-    cell_new = cell_of<FOLD>(c, px, py, pz);
-    const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + cell_new), __ldg(w_t + cell_old)), deb);
-    // accept if dE < 0; else if dE < 17 and log(u) < -dE (log_floor decides
-    // without the logarithm for all but ~1 % of trials; see trial_f)
-    bool acc = dE < 0.0f;
     const float u = u01(aw);
-    const bool near = !acc && dE < 17.0f && -dE > log_floor(u);
-    if (__any_sync(0xffffffffu, near)) acc = acc || (near && log_f(u) < -dE);
+    bool acc = false;
+    cell_old = cell_new = 0;
+    // the omega span rejects most trials before the folds and gathers (see trial_lean)
+    if (__any_sync(0xffffffffu, maybe_accepted(deb, span, log_floor(u)))) {
+        cell_old = cell_of<FOLD>(c, x, y, z);
+        cell_new = cell_of<FOLD>(c, px, py, pz);
+        const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + cell_new), __ldg(w_t + cell_old)), deb);
+        acc = dE < 0.0f;
+        const bool near = !acc && -dE > log_floor(u);
+        if (__any_sync(0xffffffffu, near)) acc = acc || (near && log_f(u) < -dE);
+    }
     return acc;
 }
 
@@ -1045,6 +1070,7 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
         float* const PZ = S->z;
         const uint32_t* const CID = S->chain_id;
         const float* const OM = S->omega;
+        const float span = S->omega_span;
         const int NCi = (int)S->n_cells;
         const ArchDev* Ap = t.arch;
         const int L = Ap->length;
@@ -1101,8 +1127,8 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
                 float fz = __fmaf_rn(__fsub_rn(lz, ze), c.k2, 0.0f);
                 add_bond(c.k2, xe, ye, ze, xo, yo, zo, fx, fy, fz);
                 float px, py, pz;
-                acc_e = trial_leanm<FOLD>(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), OM + toff_e,
-                                   px, py, pz, ce_old, ce_new) &&
+                acc_e = trial_leanm<FOLD>(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), span,
+                                          OM + toff_e, px, py, pz, ce_old, ce_new) &&
                         live;
                 xe = acc_e ? px : xe;
                 ye = acc_e ? py : ye;
@@ -1125,8 +1151,8 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
                 float fz = __fmaf_rn(__fsub_rn(ze, zo), c.k2, 0.0f);
                 add_bond(c.k2, xo, yo, zo, rx, ry, rz, fx, fy, fz);
                 float px, py, pz;
-                acc_o = trial_leanm<FOLD>(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), OM + toff_o,
-                                   px, py, pz, co_old, co_new) &&
+                acc_o = trial_leanm<FOLD>(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), span,
+                                          OM + toff_o, px, py, pz, co_old, co_new) &&
                         live;
                 xo = acc_o ? px : xo;
                 yo = acc_o ? py : yo;
@@ -1198,7 +1224,7 @@ __device__ __forceinline__ double omega_of_cell(int nt, const uint32_t* cnt, flo
 template <int NT, bool FUSED>
 __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, float scale, bool lit, bool upd,
                                              bool c16, const uint32_t* src32, float* W, const float* cf,
-                                             unsigned long long* avg) {
+                                             unsigned long long* avg, float& wmax, float& wmin) {
     constexpr int M = NT > 0 ? NT : kMaxTypes;
     const int nt = NT > 0 ? NT : n;
     const uint16_t* src16 = reinterpret_cast<const uint16_t*>(src32);
@@ -1216,6 +1242,10 @@ __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, fl
 #pragma unroll
     for (int t = 0; t < M; ++t) {
         if (t < nt && upd) W[t * NC + cell] = w[t];
+        if (t < nt) {
+            wmax = fmaxf(wmax, w[t]);  // fmaxf / fminf skip NaN
+            wmin = fminf(wmin, w[t]);
+        }
     }
     return ef;
 }
@@ -1225,7 +1255,7 @@ __device__ __forceinline__ double field_cell(int n, int64_t cell, int64_t NC, fl
 template <int NT, bool FUSED>
 __device__ __forceinline__ double field_cells4(int64_t cell, int64_t NC, float scale, bool lit, bool upd,
                                                const uint32_t* src32, float* W, const float* cf,
-                                               unsigned long long* avg) {
+                                               unsigned long long* avg, float& wmax, float& wmin) {
     uint4 cv[NT];
     float4 wv[NT];
 #pragma unroll
@@ -1257,6 +1287,8 @@ __device__ __forceinline__ double field_cells4(int64_t cell, int64_t NC, float s
         ef += omega_of_cell<NT>(NT, cnt, scale, lit, upd, w, cf);
 #pragma unroll
         for (int u = 0; u < NT; ++u) {
+            wmax = fmaxf(wmax, w[u]);
+            wmin = fminf(wmin, w[u]);
             if (l == 0) wv[u].x = w[u];
             else if (l == 1) wv[u].y = w[u];
             else if (l == 2) wv[u].z = w[u];
@@ -1315,10 +1347,21 @@ __device__ void close_system(SysDev* S, const double* part, int count, int mode,
     __syncthreads();
 }
 
+// Order-preserving integer key of a non-NaN float (for atomicMax / atomicMin)
+// and its inverse.
+__device__ __forceinline__ uint32_t ord_key(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float ord_val(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
 template <bool FUSED, int NT>
 __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ tiles, int n_tiles, int force_update,
                                                 double* __restrict__ ef_part, int close_mode) {
     __shared__ double s_ef[32];
+    __shared__ float s_mx[32], s_mn[32];
     __shared__ unsigned long long s_acc[32];
     __shared__ float cf[kMaxTypes * kMaxTypes];
     __shared__ int s_last;
@@ -1342,21 +1385,39 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
         // the fused sweep samples the time-averaged density at every avg_every-th sweep
         unsigned long long* avg = FUSED && S->avg && S->avg_every && (sweep % S->avg_every) == 0u ? S->avg : nullptr;
         double ef = 0.0;
+        float wmax = -INFINITY, wmin = INFINITY;  // omega of the tile's cells (new or kept)
         const int64_t end = t.cell0 + t.n_cells;
         if (NT > 0 && !c16 && (NC & 3) == 0 && (t.cell0 & 3) == 0 && (t.n_cells & 3) == 0) {
             for (int64_t cell = t.cell0 + 4 * tid; cell < end; cell += 4 * T)
-                ef += field_cells4<(NT > 0 ? NT : 1), FUSED>(cell, NC, scale, lit, upd, src32, W, cf, avg);
+                ef += field_cells4<(NT > 0 ? NT : 1), FUSED>(cell, NC, scale, lit, upd, src32, W, cf, avg, wmax, wmin);
         } else {
             for (int64_t cell = t.cell0 + tid; cell < end; cell += T)
-                ef += field_cell<NT, FUSED>(n, cell, NC, scale, lit, upd, c16, src32, W, cf, avg);
+                ef += field_cell<NT, FUSED>(n, cell, NC, scale, lit, upd, c16, src32, W, cf, avg, wmax, wmin);
         }
         ef = warp_sum(ef);
-        if (lane == 0) s_ef[warp] = ef;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, o));
+            wmin = fminf(wmin, __shfl_xor_sync(0xffffffffu, wmin, o));
+        }
+        if (lane == 0) {
+            s_ef[warp] = ef;
+            s_mx[warp] = wmax;
+            s_mn[warp] = wmin;
+        }
         __syncthreads();
         if (tid == 0) {
             double e = 0.0;
-            for (int w = 0; w < (T + 31) / 32; ++w) e += s_ef[w];
+            for (int w = 0; w < (T + 31) / 32; ++w) {
+                e += s_ef[w];
+                wmax = fmaxf(wmax, s_mx[w]);
+                wmin = fminf(wmin, s_mn[w]);
+            }
             ef_part[ti] = e;
+            if (wmax >= wmin) {  // the tile held a non-NaN omega
+                atomicMax(&S->om_max_key, ord_key(wmax));
+                atomicMin(&S->om_min_key, ord_key(wmin));
+            }
             if (close_mode) {
                 // publish the partial, then count the tile; the block that
                 // finishes a system's last tile closes it (no waiting)
@@ -1368,6 +1429,14 @@ __global__ void __launch_bounds__(256) k_field(const FieldTile* __restrict__ til
         __syncthreads();
         if (close_mode && s_last) {
             __threadfence();
+            if (tid == 0) {
+                // every tile of the system has folded its omega in: publish the
+                // span (+inf when no bound is known) and reset the keys
+                const uint32_t kx = atomicExch(&S->om_max_key, 0u);
+                const uint32_t kn = atomicExch(&S->om_min_key, 0xFFFFFFFFu);
+                const float span = kx >= kn ? __fsub_rn(ord_val(kx), ord_val(kn)) : INFINITY;
+                S->omega_span = span >= 0.0f ? span : INFINITY;  // NaN (inf - inf): no bound
+            }
             close_system(S, ef_part + t.first_tile, t.n_tiles_sys, close_mode, s_acc, s_ef);
             if (tid == 0) S->field_done = 0u;
         }
@@ -1991,9 +2060,10 @@ __global__ void __launch_bounds__(256) k_field_noalloc(const uint32_t* __restric
     const int64_t c0 = (int64_t)blockIdx.x * kNoAllocTileCells;
     const int64_t c1 = min(c0 + (int64_t)kNoAllocTileCells, p.n_cells);
     double ef = 0.0;
+    float wmax = -INFINITY, wmin = INFINITY;  // not used: the caller's omega has no span slot
     for (int64_t cell = c0 + tid; cell < c1; cell += T)
         ef += field_cell<0, false>(p.n_types, cell, p.n_cells, p.scale, p.lit != 0, true, false, counts, omega, cf,
-                                   nullptr);
+                                   nullptr, wmax, wmin);
     ef = warp_sum(ef);
     if (lane == 0) s_ef[warp] = ef;
     __syncthreads();

@@ -315,6 +315,7 @@ scmf_status scmf_checkpoint_read(scmf_system* s, const char* path) {
     d.total_moves = h.total_moves;
     d.e_field = h.e_field;
     d.e_bond_step = 0u;
+    d.omega_span = INFINITY;  // omega came from the file: no span until the next field step
     for (int i = 0; i < kSlots; ++i) d.slot_acc[i] = 0ull;
     if (h.avg_every) {
         if (!s->d_avg) RET(alloc_scratch((void**)&s->d_avg, cells * 8, s->stream));
