@@ -99,6 +99,7 @@ __global__ void k_init_coords(SysDev* __restrict__ S, const ArchDev* __restrict_
 // ------------------------------------------------------------------ sweep
 struct MoveConsts {
     float k, k2, A, R, inv_dx, inv_dy, inv_dz;
+    float span;  // SysDev::omega_span of the system (early rejection)
     int nx, ny, nz;
     bool pow2;   // every axis a power of two
     bool small;  // every axis of 2 to 256 cells (fold_magic)
@@ -107,6 +108,7 @@ struct MoveConsts {
 __device__ __forceinline__ bool is_pow2(int n) { return (n & (n - 1)) == 0; }
 
 __device__ __forceinline__ void load_fold(MoveConsts& c, const SysDev* S) {
+    c.span = S->omega_span;
     c.nx = S->nx; c.ny = S->ny; c.nz = S->nz;
     c.pow2 = is_pow2(c.nx) && is_pow2(c.ny) && is_pow2(c.nz);
     c.small = c.nx >= 2 && c.ny >= 2 && c.nz >= 2 && c.nx <= 256 && c.ny <= 256 && c.nz <= 256;
@@ -149,6 +151,19 @@ __device__ __forceinline__ void add_bond(float k2, float x, float y, float z, fl
     fz = __fmaf_rn(__fsub_rn(qz, z), k2, fz);
 }
 
+// Rejection before the omega reads.  Every field step publishes span >= the
+// largest omega_t[a] - omega_t[b] (SysDev::omega_span), so, rounding being
+// monotone, fl(w_new - w_old) >= -span and dE = fl(fl(w_new - w_old) + deb) >=
+// fl(deb - span) =: lb.  A trial with -lb <= log_floor(u) <= log_f(u) has
+// dE > 0 and log_f(u) >= -dE: the Metropolis test below rejects it whatever
+// omega holds (and a NaN bound or energy rejects, as the test does).  At the
+// benchmark acceptance (~0.5 %) about 2 % of trials pass this bound, so about
+// half of the warps skip the cell folds, the two gathers and their L2 round
+// trip altogether; the outcome of every trial is the oracle's.
+__device__ __forceinline__ bool maybe_accepted(float deb, float span, float lf) {
+    return -__fsub_rn(deb, span) > lf;
+}
+
 // The trial of a bead at (x,y,z) with bond force f.  With d = A f + R xi the
 // displacement, the reference's bonded energy change plus smart-MC correction
 // equals (A c / 4)(c |d|^2 - 2 f.d), c = 2k deg (the force at p + d is
@@ -170,19 +185,21 @@ __device__ __forceinline__ bool trial_f(const MoveConsts& c, float x, float y, f
     const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
     const float fd = __fmaf_rn(fx, dx, __fmaf_rn(fy, dy, __fmul_rn(fz, dz)));
     const float deb = __fmul_rn(ac4, __fmaf_rn(cc, d2, __fmul_rn(-2.0f, fd)));
-    const int c_old = cell_of<FOLD>(c, x, y, z);
-    const int c_new = cell_of<FOLD>(c, px, py, pz);
-    const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + c_new), __ldg(w_t + c_old)), deb);
-    // log(u) >= -23 ln2 > -17 for every u the generator yields: dE >= 17 rejects
-    // without the logarithm.  Below that, log_f(u) >= log_floor(u) for every
-    // such u, so -dE <= log_floor(u) rejects without it too (same outcome).
-    bool acc;
-    if (dE < 0.0f) {
-        acc = true;
-    } else if (dE < 17.0f) {
-        acc = -dE > log_floor(u01(aw)) && log_f(u01(aw)) < -dE;  // u recomputed: no register held across
-    } else {
-        acc = false;
+    // Trials that the omega span already rejects skip the folds and gathers
+    // (maybe_accepted; same outcome).  Otherwise: log(u) >= -23 ln2 > -17 for
+    // every u the generator yields, so dE >= 17 rejects without the logarithm;
+    // below that, log_f(u) >= log_floor(u) for every such u, so
+    // -dE <= log_floor(u) rejects without it too (same outcome).
+    bool acc = false;
+    int c_old = 0, c_new = 0;
+    if (maybe_accepted(deb, c.span, log_floor(u01(aw)))) {
+        c_old = cell_of<FOLD>(c, x, y, z);
+        c_new = cell_of<FOLD>(c, px, py, pz);
+        const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + c_new), __ldg(w_t + c_old)), deb);
+        if (dE < 0.0f)
+            acc = true;
+        else if (dE < 17.0f)
+            acc = -dE > log_floor(u01(aw)) && log_f(u01(aw)) < -dE;  // u recomputed: no register held across
     }
     cell_old = c_old;
     cell_new = c_new;
@@ -833,18 +850,6 @@ constexpr int kLeanThreads = 896;
 constexpr int kLeanCopies = 8;
 constexpr size_t kLeanSmem = (size_t)SCMF_NORMAL_SEGS * kLeanCopies * sizeof(float4);
 
-// Rejection before the omega reads.  Every field step publishes span >= the
-// largest omega_t[a] - omega_t[b] (SysDev::omega_span), so, rounding being
-// monotone, fl(w_new - w_old) >= -span and dE = fl(fl(w_new - w_old) + deb) >=
-// fl(deb - span) =: lb.  A trial with -lb <= log_floor(u) <= log_f(u) has
-// dE > 0 and log_f(u) >= -dE: the Metropolis test below rejects it whatever
-// omega holds (and a NaN bound or energy rejects, as the test does).  At the
-// benchmark acceptance (~0.5 %) about 2 % of trials pass this bound, so about
-// half of the warps skip the cell folds, the two gathers and their L2 round
-// trip altogether; the outcome of every trial is the oracle's.
-__device__ __forceinline__ bool maybe_accepted(float deb, float span, float lf) {
-    return -__fsub_rn(deb, span) > lf;
-}
 
 __device__ __forceinline__ bool trial_lean(const MoveConsts& c, float x, float y, float z, float fx, float fy,
                                            float fz, float cc, float ac4, float n0, float n1, float n2, uint32_t aw,
