@@ -154,7 +154,7 @@ __device__ __forceinline__ void add_bond(float k2, float x, float y, float z, fl
 // Rejection before the omega reads.  Every field step publishes span >= the
 // largest omega_t[a] - omega_t[b] (SysDev::omega_span), so, rounding being
 // monotone, fl(w_new - w_old) >= -span and dE = fl(fl(w_new - w_old) + deb) >=
-// fl(deb - span) =: lb.  A trial with -lb <= log_floor(u) <= log_f(u) has
+// fl(deb - span) =: lb.  A trial with -lb <= log_lower(u) <= log_f(u) has
 // dE > 0 and log_f(u) >= -dE: the Metropolis test below rejects it whatever
 // omega holds (and a NaN bound or energy rejects, as the test does).  At the
 // benchmark acceptance (~0.5 %) about 2 % of trials pass this bound, so about
@@ -188,18 +188,18 @@ __device__ __forceinline__ bool trial_f(const MoveConsts& c, float x, float y, f
     // Trials that the omega span already rejects skip the folds and gathers
     // (maybe_accepted; same outcome).  Otherwise: log(u) >= -23 ln2 > -17 for
     // every u the generator yields, so dE >= 17 rejects without the logarithm;
-    // below that, log_f(u) >= log_floor(u) for every such u, so
-    // -dE <= log_floor(u) rejects without it too (same outcome).
+    // below that, log_f(u) >= log_lower(u) for every such u, so
+    // -dE <= log_lower(u) rejects without it too (same outcome).
     bool acc = false;
     int c_old = 0, c_new = 0;
-    if (maybe_accepted(deb, c.span, log_floor(u01(aw)))) {
+    if (maybe_accepted(deb, c.span, log_lower(u01(aw)))) {
         c_old = cell_of<FOLD>(c, x, y, z);
         c_new = cell_of<FOLD>(c, px, py, pz);
         const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + c_new), __ldg(w_t + c_old)), deb);
         if (dE < 0.0f)
             acc = true;
         else if (dE < 17.0f)
-            acc = -dE > log_floor(u01(aw)) && log_f(u01(aw)) < -dE;  // u recomputed: no register held across
+            acc = -dE > log_lower(u01(aw)) && log_f(u01(aw)) < -dE;  // u recomputed: no register held across
     }
     cell_old = c_old;
     cell_new = c_new;
@@ -851,33 +851,41 @@ constexpr int kLeanCopies = 8;
 constexpr size_t kLeanSmem = (size_t)SCMF_NORMAL_SEGS * kLeanCopies * sizeof(float4);
 
 
-__device__ __forceinline__ bool trial_lean(const MoveConsts& c, float x, float y, float z, float fx, float fy,
+// One trial of the bead at (x, y, z) with bond force f, updated in place when
+// accepted (lanes with live false never move): the proposal, its cells and
+// the omega reads are formed only in warps where some lane passes the span
+// bound.  Returns whether the move was accepted.
+__device__ __forceinline__ bool trial_lean(const MoveConsts& c, float& x, float& y, float& z, float fx, float fy,
                                            float fz, float cc, float ac4, float n0, float n1, float n2, uint32_t aw,
-                                           float span, const float* __restrict__ w_t, float& px, float& py,
-                                           float& pz, int& cell_old, int& cell_new) {
+                                           float span, bool live, const float* __restrict__ w_t, int& cell_old,
+                                           int& cell_new) {
     const float A = c.A, R = c.R;
     const float dx = __fmaf_rn(A, fx, __fmul_rn(R, n0));
     const float dy = __fmaf_rn(A, fy, __fmul_rn(R, n1));
     const float dz = __fmaf_rn(A, fz, __fmul_rn(R, n2));
-    px = __fadd_rn(x, dx);
-    py = __fadd_rn(y, dy);
-    pz = __fadd_rn(z, dz);
     const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
     const float fd = __fmaf_rn(fx, dx, __fmaf_rn(fy, dy, __fmul_rn(fz, dz)));
     const float deb = __fmul_rn(ac4, __fmaf_rn(cc, d2, __fmul_rn(-2.0f, fd)));
     const float u = u01(aw);
     bool acc = false;
     cell_old = cell_new = 0;
-    if (__any_sync(0xffffffffu, maybe_accepted(deb, span, log_floor(u)))) {
+    if (__any_sync(0xffffffffu, maybe_accepted(deb, span, log_lower(u)))) {
+        const float px = __fadd_rn(x, dx), py = __fadd_rn(y, dy), pz = __fadd_rn(z, dz);
         cell_old = cell_of<0>(c, x, y, z);
         cell_new = cell_of<0>(c, px, py, pz);
         const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + cell_new), __ldg(w_t + cell_old)), deb);
-        // accept if dE < 0; else if log(u) < -dE (log_floor decides without the
-        // logarithm for all but ~1 % of trials; see trial_f; dE >= 17 fails
-        // -dE > log_floor(u) >= -23 ln2 - 2^-10)
+        // accept if dE < 0; else if log(u) < -dE (log_lower decides without the
+        // logarithm for all but a few trials in a thousand; dE >= 17 fails
+        // -dE > log_lower(u) >= -16, so no separate bound is needed)
         acc = dE < 0.0f;
-        const bool near = !acc && -dE > log_floor(u);
+        const bool near = !acc && -dE > log_lower(u);
         if (__any_sync(0xffffffffu, near)) acc = acc || (near && log_f(u) < -dE);
+        acc = acc && live;
+        if (acc) {
+            x = px;
+            y = py;
+            z = pz;
+        }
     }
     return acc;
 }
@@ -965,13 +973,8 @@ __global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysCon
                 float fy = __fmaf_rn(__fsub_rn(ly, ye), c.k2, 0.0f);
                 float fz = __fmaf_rn(__fsub_rn(lz, ze), c.k2, 0.0f);
                 add_bond(c.k2, xe, ye, ze, xo, yo, zo, fx, fy, fz);
-                float px, py, pz;
-                acc_e = trial_lean(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), span,
-                                   sc.omega + toff_e, px, py, pz, ce_old, ce_new) &&
-                        live;
-                xe = acc_e ? px : xe;
-                ye = acc_e ? py : ye;
-                ze = acc_e ? pz : ze;
+                acc_e = trial_lean(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), span, live,
+                                   sc.omega + toff_e, ce_old, ce_new);
                 mv_e = acc_e && ce_new != ce_old;
             }
             // odd bead 2t+1: bonds to 2t (moved) and 2t+2 (lane + 1's moved even bead; the bead itself at the end)
@@ -989,13 +992,8 @@ __global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysCon
                 float fy = __fmaf_rn(__fsub_rn(ye, yo), c.k2, 0.0f);
                 float fz = __fmaf_rn(__fsub_rn(ze, zo), c.k2, 0.0f);
                 add_bond(c.k2, xo, yo, zo, rx, ry, rz, fx, fy, fz);
-                float px, py, pz;
-                acc_o = trial_lean(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), span,
-                                   sc.omega + toff_o, px, py, pz, co_old, co_new) &&
-                        live;
-                xo = acc_o ? px : xo;
-                yo = acc_o ? py : yo;
-                zo = acc_o ? pz : zo;
+                acc_o = trial_lean(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), span, live,
+                                   sc.omega + toff_o, co_old, co_new);
                 mv_o = acc_o && co_new != co_old;
             }
             nacc += (acc_e ? 1u : 0u) + (acc_o ? 1u : 0u);
@@ -1024,17 +1022,14 @@ __global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysCon
 // 96 registers (no spill) the 256-system mix ran 7.39e10 bead-moves/s against
 // 7.00e10 with k_sweep_reg (80-88 registers spilled and lost).
 template <int FOLD>
-__device__ __forceinline__ bool trial_leanm(const MoveConsts& c, float x, float y, float z, float fx, float fy,
+__device__ __forceinline__ bool trial_leanm(const MoveConsts& c, float& x, float& y, float& z, float fx, float fy,
                                            float fz, float cc, float ac4, float n0, float n1, float n2, uint32_t aw,
-                                           float span, const float* __restrict__ w_t, float& px, float& py,
-                                           float& pz, int& cell_old, int& cell_new) {
+                                           float span, bool live, const float* __restrict__ w_t, int& cell_old,
+                                           int& cell_new) {
     const float A = c.A, R = c.R;
     const float dx = __fmaf_rn(A, fx, __fmul_rn(R, n0));
     const float dy = __fmaf_rn(A, fy, __fmul_rn(R, n1));
     const float dz = __fmaf_rn(A, fz, __fmul_rn(R, n2));
-    px = __fadd_rn(x, dx);
-    py = __fadd_rn(y, dy);
-    pz = __fadd_rn(z, dz);
     const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
     const float fd = __fmaf_rn(fx, dx, __fmaf_rn(fy, dy, __fmul_rn(fz, dz)));
     const float deb = __fmul_rn(ac4, __fmaf_rn(cc, d2, __fmul_rn(-2.0f, fd)));
@@ -1042,13 +1037,20 @@ __device__ __forceinline__ bool trial_leanm(const MoveConsts& c, float x, float 
     bool acc = false;
     cell_old = cell_new = 0;
     // the omega span rejects most trials before the folds and gathers (see trial_lean)
-    if (__any_sync(0xffffffffu, maybe_accepted(deb, span, log_floor(u)))) {
+    if (__any_sync(0xffffffffu, maybe_accepted(deb, span, log_lower(u)))) {
+        const float px = __fadd_rn(x, dx), py = __fadd_rn(y, dy), pz = __fadd_rn(z, dz);
         cell_old = cell_of<FOLD>(c, x, y, z);
         cell_new = cell_of<FOLD>(c, px, py, pz);
         const float dE = __fadd_rn(__fsub_rn(__ldg(w_t + cell_new), __ldg(w_t + cell_old)), deb);
         acc = dE < 0.0f;
-        const bool near = !acc && -dE > log_floor(u);
+        const bool near = !acc && -dE > log_lower(u);
         if (__any_sync(0xffffffffu, near)) acc = acc || (near && log_f(u) < -dE);
+        acc = acc && live;
+        if (acc) {
+            x = px;
+            y = py;
+            z = pz;
+        }
     }
     return acc;
 }
@@ -1131,13 +1133,8 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
                 float fy = __fmaf_rn(__fsub_rn(ly, ye), c.k2, 0.0f);
                 float fz = __fmaf_rn(__fsub_rn(lz, ze), c.k2, 0.0f);
                 add_bond(c.k2, xe, ye, ze, xo, yo, zo, fx, fy, fz);
-                float px, py, pz;
                 acc_e = trial_leanm<FOLD>(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), span,
-                                          OM + toff_e, px, py, pz, ce_old, ce_new) &&
-                        live;
-                xe = acc_e ? px : xe;
-                ye = acc_e ? py : ye;
-                ze = acc_e ? pz : ze;
+                                          live, OM + toff_e, ce_old, ce_new);
                 mv_e = acc_e && ce_new != ce_old;
             }
             // odd bead 2t+1: bonds to 2t (moved) and 2t+2 (lane + 1's moved even bead; the bead itself at the end)
@@ -1155,13 +1152,8 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
                 float fy = __fmaf_rn(__fsub_rn(ye, yo), c.k2, 0.0f);
                 float fz = __fmaf_rn(__fsub_rn(ze, zo), c.k2, 0.0f);
                 add_bond(c.k2, xo, yo, zo, rx, ry, rz, fx, fy, fz);
-                float px, py, pz;
                 acc_o = trial_leanm<FOLD>(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), span,
-                                          OM + toff_o, px, py, pz, co_old, co_new) &&
-                        live;
-                xo = acc_o ? px : xo;
-                yo = acc_o ? py : yo;
-                zo = acc_o ? pz : zo;
+                                          live, OM + toff_o, co_old, co_new);
                 mv_o = acc_o && co_new != co_old;
             }
             nacc += (acc_e ? 1u : 0u) + (acc_o ? 1u : 0u);

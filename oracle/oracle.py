@@ -89,8 +89,8 @@ def lib():
     L.orc_philox4x32_10.argtypes = [u32p, u32p, u32p]
     L.orc_logf.restype = C.c_float
     L.orc_logf.argtypes = [C.c_float]
-    L.orc_log_floor_violations.restype = C.c_long
-    L.orc_log_floor_violations.argtypes = [C.c_float, C.c_float, C.POINTER(C.c_float)]
+    L.orc_log_lower_violations.restype = C.c_long
+    L.orc_log_lower_violations.argtypes = [C.c_float, C.c_float, C.POINTER(C.c_float)]
     L.orc_normal.restype = C.c_float
     L.orc_normal.argtypes = [C.c_uint32]
     L.orc_normals3.argtypes = [u32p, f32p, f32p, f32p]

@@ -65,16 +65,16 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
 float orc_u01(uint32_t w) { return 2.0f - u2f(0x3F800000u | (w >> 9)); }
 
 /* Test helper for the kernels' early Metropolis reject: over all 2^23 values
- * orc_u01 yields, counts those whose orc_logf lies below the exponent bound
- * e * ln2_f - slack (one fma, as the kernel computes it) and returns the
- * smallest margin log - bound in *min_margin. */
-long orc_log_floor_violations(float ln2_f, float slack, float* min_margin) {
+ * orc_u01 yields, counts those whose orc_logf lies below the bound
+ * fma((float)bits(u), c1, c0) (a conversion and one fma, as the kernels'
+ * log_lower computes it) and returns the smallest margin log - bound in
+ * *min_margin. */
+long orc_log_lower_violations(float c1, float c0, float* min_margin) {
     long bad = 0;
     float mm = 1e30f;
     for (uint32_t j = 0; j < (1u << 23); ++j) {
         const float u = orc_u01(j << 9);
-        const int e = (int)(f2u(u) >> 23) - 127;
-        const float lo = fmaf((float)e, ln2_f, -slack);
+        const float lo = fmaf((float)f2u(u), c1, c0);
         const float l = orc_logf(u);
         if (!(l >= lo)) ++bad;
         if (l - lo < mm) mm = l - lo;

@@ -91,7 +91,7 @@ int  orc_analyze(const orc_system* s, int arch, double* out);
 /* math building blocks (exported for known-answer tests) */
 void  orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 float orc_logf(float x);
-long orc_log_floor_violations(float ln2_f, float slack, float* min_margin);
+long orc_log_lower_violations(float c1, float c0, float* min_margin);
 float orc_normal(uint32_t w);   /* one standard normal from one word (inverse CDF) */
 void  orc_normals3(const uint32_t w[4], float* n0, float* n1, float* n2);
 float orc_u01(uint32_t w);

@@ -224,21 +224,26 @@ def test_scmf0_mean_omega_matches_reference_density_files():
     assert w == pytest.approx(scmf0_reference([0.125, 0.75, 0.125], xn, 32), abs=1e-6)
 
 
-def test_log_floor_bounds_every_uniform():
-    """The kernels reject a move without the logarithm when -dE <= e ln2 -
-    slack (u in [2^e, 2^(e+1))).  That gives the oracle's outcome only if the
-    bound lies at or below log_f(u) for every u the generator yields: checked
-    over all 2^23 of them with the constants of the device source."""
+def test_log_lower_bounds_every_uniform():
+    """The kernels reject a move without the logarithm (and without reading
+    omega, with the omega span) when -dE <= log_lower(u), a bound linear in
+    the bits of u.  That gives the oracle's outcome only if the bound lies at
+    or below log_f(u) for every u the generator yields: checked over all 2^23
+    of them with the constants of the device source."""
     import ctypes as C
     import re
     src = open(os.path.join(os.path.dirname(GOLDEN), "..", "new_arch_b200", "csrc", "scmf_math.cuh")).read()
-    m = re.search(r"log_floor\(float u\).*?__fmaf_rn\(__int2float_rn\(e\), ([0-9a-fx.p+-]+)f, -([0-9a-fx.p+-]+)f\)", src, re.S)
-    assert m, "log_floor not found"
-    ln2_f, slack = float.fromhex(m.group(1)), float.fromhex(m.group(2))
+    m = re.search(r"log_lower\(float u\).*?__fmaf_rn\(__uint2float_rn\(__float_as_uint\(u\)\), ([0-9a-fx.p+-]+)f, "
+                  r"(-?[0-9a-fx.p+-]+)f\)", src, re.S)
+    assert m, "log_lower not found"
+    c1, c0 = float.fromhex(m.group(1)), float.fromhex(m.group(2))
     mm = C.c_float()
-    bad = orc.lib().orc_log_floor_violations(ln2_f, slack, C.byref(mm))
+    bad = orc.lib().orc_log_lower_violations(c1, c0, C.byref(mm))
     assert bad == 0
-    assert 0.0 < mm.value < 2 * slack  # tight enough to skip most logarithms
+    assert 0.0 < mm.value < 1e-3  # tight: a slack of 2^-12 and no more
+    # the bound stays above -17, so dE >= 17 still rejects through it
+    u_min = np.float32(2.0 ** -23)
+    assert np.float32(u_min.view(np.uint32)) * np.float32(c1) + np.float32(c0) > -17.0
 
 
 def test_multiply_high_fold_identity():
