@@ -518,6 +518,8 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
             la.n_chains = archs[a].n_chains;
             la.chain0 = archs[a].chain_base;
             la.bead0 = (int32_t)archs[a].bead_base;
+            la.rng0 = archs[a].rng_base;  // chain_id[chain_base + c] = rng_base + c (storage order is never permuted)
+            la.pad = 0;
         }
     } else {
         if (p->seed != spec.p.seed) p->one_seed = false;

@@ -199,6 +199,8 @@ struct LeanArch {
     int32_t n_chains;
     int32_t chain0;        // first chain (index into chain_id)
     int32_t bead0;         // first bead
+    int32_t rng0;          // random-stream id of the first chain (chain_id[chain0 + c] = rng0 + c)
+    int32_t pad;
 };
 constexpr int kLeanMaxArch = 4;
 

@@ -931,37 +931,37 @@ __global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysCon
         const float cc_o = last ? sc.cdeg[1] : sc.cdeg[2], ac4_o = last ? sc.ac4deg[1] : sc.ac4deg[2];
         const int toff_e = (int)__ldg(sc.arch[a].types + be) * (int)sc.n_cells;
         const int toff_o = (int)__ldg(sc.arch[a].types + bo) * (int)sc.n_cells;
+        // a chain end's missing bond: the shuffles below return the lane's own
+        // bead there, and these zero spring constants make its term +-0
+        const float k2_l = first ? 0.0f : sc.k2, k2_r = last ? 0.0f : sc.k2;
         const int nch = sc.arch[a].n_chains;
-        const int bead0 = sc.arch[a].bead0, chain0 = sc.arch[a].chain0;
+        const int bead0 = sc.arch[a].bead0;
+        const uint32_t rng0 = (uint32_t)sc.arch[a].rng0;
         const int groups = (nch + cpw - 1) >> (5 - lg);
         // the pairs and chain id of the warp's next group are loaded one group
         // ahead, so the DRAM latency overlaps this group's trials
         float2 nvx = make_float2(0.0f, 0.0f), nvy = nvx, nvz = nvx;
-        uint32_t ngc = 0u;
         auto fetch = [&](int grp) {
             const int ch = min(grp * cpw + cs, nch - 1);
             const int gn = bead0 + ch * L + be;
             nvx = __ldcs(reinterpret_cast<const float2*>(sc.x + gn));
             nvy = __ldcs(reinterpret_cast<const float2*>(sc.y + gn));
             nvz = __ldcs(reinterpret_cast<const float2*>(sc.z + gn));
-            ngc = __ldg(sc.chain_id + chain0 + ch);
         };
         if (gw < groups) fetch(gw);
         for (int grp = gw; grp < groups; grp += nw) {  // warp-uniform bounds
             const int chain = grp * cpw + cs;
             const bool live = chain < nch;
-            const int g = bead0 + (live ? chain : nch - 1) * L + be;
+            const int chc = live ? chain : nch - 1;
+            const int g = bead0 + chc * L + be;
             const float2 vx = nvx, vy = nvy, vz = nvz;
-            const uint32_t gc = ngc;
+            const uint32_t gc = rng0 + (uint32_t)chc;  // storage order is the stream order
             if (grp + nw < groups) fetch(grp + nw);
             float xe = vx.x, xo = vx.y, ye = vy.x, yo = vy.y, ze = vz.x, zo = vz.y;
             // even bead 2t: bonds to 2t-1 (lane - 1's odd bead; the bead itself at the chain start) and 2t+1
-            float lx = __shfl_up_sync(0xffffffffu, xo, 1);
-            float ly = __shfl_up_sync(0xffffffffu, yo, 1);
-            float lz = __shfl_up_sync(0xffffffffu, zo, 1);
-            lx = first ? xe : lx;
-            ly = first ? ye : ly;
-            lz = first ? ze : lz;
+            const float lx = __shfl_up_sync(0xffffffffu, xo, 1, tpc);
+            const float ly = __shfl_up_sync(0xffffffffu, yo, 1, tpc);
+            const float lz = __shfl_up_sync(0xffffffffu, zo, 1, tpc);
             const uint4 w = philox4x32_10(make_uint4(gc, (uint32_t)be, step, 0u), keys);
             const uint4 wo = philox4x32_10(make_uint4(gc, (uint32_t)bo, step, 0u), keys);
             float n0, n1, n2;
@@ -969,21 +969,18 @@ __global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysCon
             bool acc_e, mv_e;
             int ce_old, ce_new;
             {
-                float fx = __fmaf_rn(__fsub_rn(lx, xe), c.k2, 0.0f);
-                float fy = __fmaf_rn(__fsub_rn(ly, ye), c.k2, 0.0f);
-                float fz = __fmaf_rn(__fsub_rn(lz, ze), c.k2, 0.0f);
+                float fx = __fmaf_rn(__fsub_rn(lx, xe), k2_l, 0.0f);
+                float fy = __fmaf_rn(__fsub_rn(ly, ye), k2_l, 0.0f);
+                float fz = __fmaf_rn(__fsub_rn(lz, ze), k2_l, 0.0f);
                 add_bond(c.k2, xe, ye, ze, xo, yo, zo, fx, fy, fz);
                 acc_e = trial_lean(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), span, live,
                                    sc.omega + toff_e, ce_old, ce_new);
                 mv_e = acc_e && ce_new != ce_old;
             }
             // odd bead 2t+1: bonds to 2t (moved) and 2t+2 (lane + 1's moved even bead; the bead itself at the end)
-            float rx = __shfl_down_sync(0xffffffffu, xe, 1);
-            float ry = __shfl_down_sync(0xffffffffu, ye, 1);
-            float rz = __shfl_down_sync(0xffffffffu, ze, 1);
-            rx = last ? xo : rx;
-            ry = last ? yo : ry;
-            rz = last ? zo : rz;
+            const float rx = __shfl_down_sync(0xffffffffu, xe, 1, tpc);
+            const float ry = __shfl_down_sync(0xffffffffu, ye, 1, tpc);
+            const float rz = __shfl_down_sync(0xffffffffu, ze, 1, tpc);
             normals3<kLeanCopies>(wo, tab, n0, n1, n2);
             bool acc_o, mv_o;
             int co_old, co_new;
@@ -991,7 +988,7 @@ __global__ void __maxnreg__(72) k_sweep_lean(const PhiloxKeys keys, const SysCon
                 float fx = __fmaf_rn(__fsub_rn(xe, xo), c.k2, 0.0f);
                 float fy = __fmaf_rn(__fsub_rn(ye, yo), c.k2, 0.0f);
                 float fz = __fmaf_rn(__fsub_rn(ze, zo), c.k2, 0.0f);
-                add_bond(c.k2, xo, yo, zo, rx, ry, rz, fx, fy, fz);
+                add_bond(k2_r, xo, yo, zo, rx, ry, rz, fx, fy, fz);
                 acc_o = trial_lean(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), span, live,
                                    sc.omega + toff_o, co_old, co_new);
                 mv_o = acc_o && co_new != co_old;
