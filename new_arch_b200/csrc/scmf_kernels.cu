@@ -1072,7 +1072,6 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
         float* const PX = S->x;
         float* const PY = S->y;
         float* const PZ = S->z;
-        const uint32_t* const CID = S->chain_id;
         const float* const OM = S->omega;
         const float span = S->omega_span;
         const int NCi = (int)S->n_cells;
@@ -1088,37 +1087,38 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
         const float cc_o = last ? S->cdeg[1] : S->cdeg[2], ac4_o = last ? S->ac4deg[1] : S->ac4deg[2];
         const int toff_e = (int)__ldg(Ap->types + be) * NCi;
         const int toff_o = (int)__ldg(Ap->types + bo) * NCi;
+        // a chain end's missing bond: the shuffles below return the lane's own
+        // bead there, and these zero spring constants make its term +-0
+        const float k2_l = first ? 0.0f : c.k2, k2_r = last ? 0.0f : c.k2;
+        // random-stream id of the tile's first chain (storage order is the stream order)
+        const uint32_t rng0 = (uint32_t)(Ap->rng_base + (t.chain0 - Ap->chain_base));
         const int nch = t.n_chains;
         const int stride = nwarps * cpw;
         unsigned nacc = 0;
         // the pair and chain id of the next iteration are loaded one iteration
         // ahead, so the DRAM latency overlaps this iteration's trials
         float2 nvx = make_float2(0.0f, 0.0f), nvy = nvx, nvz = nvx;
-        uint32_t ngc = 0u;
         auto fetch = [&](int cb) {
             const int ch = min(cb + cs, nch - 1);
             const int gn = (int)t.bead0 + ch * L + be;
             nvx = __ldcs(reinterpret_cast<const float2*>(PX + gn));
             nvy = __ldcs(reinterpret_cast<const float2*>(PY + gn));
             nvz = __ldcs(reinterpret_cast<const float2*>(PZ + gn));
-            ngc = __ldg(CID + t.chain0 + ch);
         };
         if (warp * cpw < nch) fetch(warp * cpw);
         for (int cbase = warp * cpw; cbase < nch; cbase += stride) {  // warp-uniform bounds
             const int chain = cbase + cs;
             const bool live = chain < nch;
-            const int g = (int)t.bead0 + (live ? chain : nch - 1) * L + be;
+            const int chc = live ? chain : nch - 1;
+            const int g = (int)t.bead0 + chc * L + be;
             const float2 vx = nvx, vy = nvy, vz = nvz;
-            const uint32_t gc = ngc;
+            const uint32_t gc = rng0 + (uint32_t)chc;
             if (cbase + stride < nch) fetch(cbase + stride);
             float xe = vx.x, xo = vx.y, ye = vy.x, yo = vy.y, ze = vz.x, zo = vz.y;
             // even bead 2t: bonds to 2t-1 (lane - 1's odd bead; the bead itself at the chain start) and 2t+1
-            float lx = __shfl_up_sync(0xffffffffu, xo, 1);
-            float ly = __shfl_up_sync(0xffffffffu, yo, 1);
-            float lz = __shfl_up_sync(0xffffffffu, zo, 1);
-            lx = first ? xe : lx;
-            ly = first ? ye : ly;
-            lz = first ? ze : lz;
+            const float lx = __shfl_up_sync(0xffffffffu, xo, 1, tpc);
+            const float ly = __shfl_up_sync(0xffffffffu, yo, 1, tpc);
+            const float lz = __shfl_up_sync(0xffffffffu, zo, 1, tpc);
             const uint4 w = philox_block<KEYS>(make_uint4(gc, (uint32_t)be, step, 0u), k0, k1, keys);
             const uint4 wo = philox_block<KEYS>(make_uint4(gc, (uint32_t)bo, step, 0u), k0, k1, keys);
             float n0, n1, n2;
@@ -1126,21 +1126,18 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
             bool acc_e, mv_e;
             int ce_old, ce_new;
             {
-                float fx = __fmaf_rn(__fsub_rn(lx, xe), c.k2, 0.0f);
-                float fy = __fmaf_rn(__fsub_rn(ly, ye), c.k2, 0.0f);
-                float fz = __fmaf_rn(__fsub_rn(lz, ze), c.k2, 0.0f);
+                float fx = __fmaf_rn(__fsub_rn(lx, xe), k2_l, 0.0f);
+                float fy = __fmaf_rn(__fsub_rn(ly, ye), k2_l, 0.0f);
+                float fz = __fmaf_rn(__fsub_rn(lz, ze), k2_l, 0.0f);
                 add_bond(c.k2, xe, ye, ze, xo, yo, zo, fx, fy, fz);
                 acc_e = trial_leanm<FOLD>(c, xe, ye, ze, fx, fy, fz, cc_e, ac4_e, n0, n1, n2, accept_word(w), span,
                                           live, OM + toff_e, ce_old, ce_new);
                 mv_e = acc_e && ce_new != ce_old;
             }
             // odd bead 2t+1: bonds to 2t (moved) and 2t+2 (lane + 1's moved even bead; the bead itself at the end)
-            float rx = __shfl_down_sync(0xffffffffu, xe, 1);
-            float ry = __shfl_down_sync(0xffffffffu, ye, 1);
-            float rz = __shfl_down_sync(0xffffffffu, ze, 1);
-            rx = last ? xo : rx;
-            ry = last ? yo : ry;
-            rz = last ? zo : rz;
+            const float rx = __shfl_down_sync(0xffffffffu, xe, 1, tpc);
+            const float ry = __shfl_down_sync(0xffffffffu, ye, 1, tpc);
+            const float rz = __shfl_down_sync(0xffffffffu, ze, 1, tpc);
             normals3(wo, s_ntab, n0, n1, n2);
             bool acc_o, mv_o;
             int co_old, co_new;
@@ -1148,7 +1145,7 @@ __global__ void __maxnreg__(96) k_sweep_leanm(const MoveTile* __restrict__ tiles
                 float fx = __fmaf_rn(__fsub_rn(xe, xo), c.k2, 0.0f);
                 float fy = __fmaf_rn(__fsub_rn(ye, yo), c.k2, 0.0f);
                 float fz = __fmaf_rn(__fsub_rn(ze, zo), c.k2, 0.0f);
-                add_bond(c.k2, xo, yo, zo, rx, ry, rz, fx, fy, fz);
+                add_bond(k2_r, xo, yo, zo, rx, ry, rz, fx, fy, fz);
                 acc_o = trial_leanm<FOLD>(c, xo, yo, zo, fx, fy, fz, cc_o, ac4_o, n0, n1, n2, accept_word(wo), span,
                                           live, OM + toff_o, co_old, co_new);
                 mv_o = acc_o && co_new != co_old;
