@@ -565,7 +565,12 @@ scmf_status scmf_system::append_plan(const scmf_tune& t, Plan* p) {
         }
         p->max_length = std::max(p->max_length, A.length);
         p->lean_ok = p->lean_ok && A.linear && A.length % 2 == 0 && A.length <= 64 && 32 % (A.length / 2) == 0;
-        if (A.linear && A.length <= 64 && 32 % ((A.length + 1) / 2) == 0) p->warp_even = p->warp_even && A.length % 2 == 0;
+        // the multi-system lean kernel reads bead pairs as float2: every warp-wise
+        // architecture must have an even length and start at an even bead (an
+        // odd-length architecture with an odd chain count before it would shift
+        // it by one); otherwise the register kernel, which checks, runs them
+        if (A.linear && A.length <= 64 && 32 % ((A.length + 1) / 2) == 0)
+            p->warp_even = p->warp_even && A.length % 2 == 0 && A.bead_base % 2 == 0;
         p->max_deg = std::max(p->max_deg, A.max_deg);
         p->linear = p->linear && A.linear;
     }

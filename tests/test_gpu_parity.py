@@ -124,6 +124,46 @@ def test_long_linear_chains(nb, lengths):
         compare_state(s, orc, f"lengths {lengths}")
 
 
+@pytest.mark.parametrize("threads", [64, 256])
+@pytest.mark.parametrize("seeds", ["one", "same_high_word", "distinct_high_words"])
+def test_chains_across_warps_key_modes(nb, threads, seeds):
+    """Lengths laid across warps (48, 24, 12, 6) beside warp-filling ones
+    (32, 16) in one batch, in every key mode and at two block sizes: each
+    system equals the oracle bit for bit."""
+    from new_arch_b200.spec import diblock_melt
+    lengths = (48, 24, 12, 6, 32, 16)
+    specs = [diblock_melt(max(3, int(7.8 * 8 * 6 * 5 / n)), n, 0.35, (8, 6, 5), 22.0, 50.0, seed=1)
+             for n in lengths]
+    for i, sp in enumerate(specs):
+        sp.seed = {"one": 55, "same_high_word": 55 + i, "distinct_high_words": 55 + (i << 33)}[seeds]
+    systems = [nb.System(sp) for sp in specs]
+    for x in systems:
+        x.init_coords()
+    b = nb.Batch(systems, tune={"beads_per_tile": 1024, "threads_move": threads})
+    b.step(4)
+    for n, sp, x in zip(lengths, specs, systems):
+        orc = oracle_for(sp)
+        orc.step(4)
+        compare_state(x, orc, f"L={n} threads={threads} seeds={seeds}")
+    b.close()
+    for x in systems:
+        x.close()
+
+
+def test_two_lengths_across_warps_one_system(nb):
+    """One system of two architectures laid across warps (48 and 24 beads)."""
+    from new_arch_b200.spec import SystemSpec, cell_units, diblock_arch, interaction_matrix
+    k, sig = cell_units()
+    spec = SystemSpec(2, 10, 8, 8, 10.0, 8.0, 8.0, interaction_matrix(2, 20.0, 50.0), 48, k, 0.5, 313,
+                      nb.HAM_SCMF0, nb.FIELD_EVERY, 32, [diblock_arch(48, 0.3, 70, sig), diblock_arch(24, 0.5, 71, sig)])
+    with nb.System(spec) as s:
+        s.init_coords()
+        orc = oracle_for(spec)
+        s.step(5)
+        orc.step(5)
+        compare_state(s, orc, "L=48 and 24")
+
+
 def test_chains_across_warps_alone(nb):
     from new_arch_b200.spec import diblock_melt
     spec = diblock_melt(700, 48, 0.3, (12, 10, 8), 25.0, 50.0, seed=48)
@@ -315,6 +355,10 @@ def test_edge_shapes(nb):
         "mixed short": [homopolymer_arch(1, 0, 300, sig), diblock_arch(2, 0.5, 200, sig),
                         diblock_arch(3, 0.34, 150, sig), homopolymer_arch(5, 1, 0, sig)],
         "one chain": [diblock_arch(32, 0.5, 1, sig)],
+        # an odd-length architecture laid across warps with an odd chain count
+        # shifts the next architecture to an odd bead: its pairs are not
+        # float2-aligned, so the register kernel (which checks) moves them
+        "odd offset": [diblock_arch(5, 0.4, 3, sig), diblock_arch(32, 0.5, 40, sig)],
         "one bead": [homopolymer_arch(1, 1, 1, sig)],
     }
     for name, archs in cases.items():
