@@ -108,9 +108,9 @@ def test_chains_across_warps(nb, threads):
 
 @pytest.mark.parametrize("lengths", [(80,), (65, 100), (48, 96, 16)])
 def test_long_linear_chains(nb, lengths):
-    """Chains longer than 64 beads take the shared-memory kernel (which keeps
-    each even bead's spare sine for its odd partner); every length in the
-    system goes through it, against the oracle bit for bit."""
+    """Chains longer than 64 beads take the shared-memory kernel (each warp's
+    chains staged with the even beads before the odd ones); every length in
+    the system goes through it, against the oracle bit for bit."""
     from new_arch_b200.spec import SystemSpec, cell_units, diblock_arch, interaction_matrix
     k, sig = cell_units()
     archs = [diblock_arch(n, 0.5, max(2, int(7.8 * 8 * 8 * 6 / n / len(lengths))), sig) for n in lengths]
