@@ -112,6 +112,12 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- helpers
+def workload_config(spec) -> dict:
+    """The workload every arm of the bench runs (both arms print the same dict)."""
+    return {"workload": WORKLOAD, "beads": spec.n_beads, "cells": spec.n_cells,
+            "l2": "inputs larger than L2 (614 MB coordinates), no flush"}
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -185,8 +191,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": done, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "beads": spec.n_beads, "cells": spec.n_cells,
-                       "parallelism": "host threads", "l2": "inputs larger than L2"},
+            "config": workload_config(spec), "run": {"parallelism": f"{threads} host threads", "sweeps_timed": done},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -286,9 +291,8 @@ def run_ours(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (random-walk chains)",
-            "config": {"workload": WORKLOAD, "beads": spec.n_beads, "cells": spec.n_cells, "sweeps_timed": args.steps,
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (614 MB coordinates), no flush"},
+            "config": workload_config(spec),
+            "run": {"parallelism": f"replicas x{world}" if world > 1 else "single GPU", "sweeps_timed": args.steps},
             "clocks": clocks, "e2e": e2e, "gpu_launches": 2 * args.steps,
             "accept_ratio": accept_ratio,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -511,9 +515,9 @@ def run_sharded(args):
         line = {"metric": METRIC, "value": spec.n_beads * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (random-walk chains)",
-                "config": {"workload": WORKLOAD, "beads": spec.n_beads, "cells": spec.n_cells,
-                           "parallelism": f"chain shards x{world}, NCCL all-reduce of the counts per sweep",
-                           "l2": "inputs larger than L2 (614 MB coordinates), no flush"},
+                "config": workload_config(spec),
+                "run": {"parallelism": f"chain shards x{world}, NCCL all-reduce of the counts per sweep",
+                        "sweeps_timed": args.steps},
                 "clocks": clocks, "gpu_launches": 2 * args.steps * 1, "mode": "sharded"}
         print(json.dumps(line), flush=True)
     return 0
