@@ -7,8 +7,11 @@
 //                                      chain are contiguous; chains are grouped
 //                                      by architecture (init_config.cu:610-629).
 //   chain_id     uint32[n_chains]     storage slot -> global chain id (the first
-//                                      Philox counter word), so chains can be reordered in space
-//                                      without changing any result.
+//                                      Philox counter word).  Storage order is the id
+//                                      order within each architecture (chain_id[chain_base
+//                                      + c] = rng_base + c), which the lean kernels use to
+//                                      compute the id instead of loading it; the other
+//                                      kernels read this table.
 //   counts[2]    uint32[n_types*n_cells] (or uint16 pairs)  per-type cell counts,
 //                                      [type][z][y][x].  counts[cur] is kept the
 //                                      grid of the positions: a fused sweep
