@@ -11,7 +11,11 @@ oracle/ref_shim/) together with oracle/ref_harness.cpp, which calls:
 * trial_move_smc_arr + add_bond_forces_arr (device_function.cu:589-717) and
   calc_delta_energy_arr + calc_delta_bonded_energy_arr (:509-588), the
   smart-MC displacement and energy change for given Gaussian numbers, against
-  the oracle's trial (closed-form bonded + smart-MC energy).
+  the oracle's trial (closed-form bonded + smart-MC energy);
+* mc_polymer_move_arr (device_function.cu:718-799), the whole sweep kernel,
+  run on the host with a seeded generator in place of cuRAND, against the
+  oracle's sweeps: equilibrium statistics (acceptance ratio, bond length,
+  beads in favoured cells) agree within statistical error.
 
 Tolerances state what FP32 against FP64 allows: folds identical except within
 1e-5 cells of a cell face; omega within 1e-6 of its largest value; the
@@ -45,6 +49,9 @@ def ref():
     L.rh_omega.argtypes = [i, i64, C.POINTER(C.c_int), C.POINTER(C.c_double), i, d, C.POINTER(C.c_double)]
     L.rh_trial.argtypes = [i, C.POINTER(C.c_int), f, i, d, d, f, d, d, d, i, i, i, i, C.POINTER(C.c_double), f,
                            C.POINTER(C.c_double)]
+    L.rh_sweeps.restype = C.c_longlong
+    L.rh_sweeps.argtypes = [i, i, C.POINTER(C.c_int), f, i, d, d, d, d, d, i, i, i, i, C.POINTER(C.c_double),
+                            C.c_uint64]
     return L
 
 
@@ -186,3 +193,82 @@ def test_trial_matches_reference(ref, case):
         assert abs(e_orc - e_total) <= 1e-5 * scale, (trial, e_orc, e_total, e_ref)
         checked += 1
     assert checked > 2500
+
+
+def _sweep_statistics(run, n_chains, L, blocks, per):
+    """Per block of `per` sweeps: the acceptance ratio, and at its end the
+    mean squared bond length and the fraction of A beads (the first half of
+    each chain) in the cells of odd x, where the field favours them."""
+    acc, b2, fav = [], [], []
+    for blk in range(blocks):
+        a, xyz = run(blk)
+        c = xyz.reshape(n_chains, L, 3).astype(np.float64)
+        acc.append(a / (per * n_chains * L))
+        b2.append(np.mean(np.sum(np.diff(c, axis=1) ** 2, axis=2)))
+        xa = np.floor(c[:, : L // 2, 0]).astype(np.int64) % 2
+        fav.append(np.mean(xa == 1))
+    return np.array(acc), np.array(b2), np.array(fav)
+
+
+def test_sweeps_match_reference_statistics(ref):
+    """The reference's whole sweep kernel, mc_polymer_move_arr
+    (device_function.cu:718-799: per chain, L trials of beads picked at random
+    with replacement, smart-MC proposals, Metropolis with exp), run on the host
+    with a seeded generator in place of cuRAND, against the oracle's
+    checkerboard sweeps of the same system: diblocks of 16 beads in a static
+    field of +-0.5 alternating cell by cell along x, opposite for A and B
+    beads.  The two update orders sample the same equilibrium, so after 400
+    sweeps their acceptance ratios, mean squared bond lengths and fractions of
+    A beads in favoured cells agree within statistical error (5 block standard
+    errors).  The oracle with the smart-MC correction dropped (a mistake
+    planted on purpose) does not."""
+    from new_arch_b200.spec import Arch, interaction_matrix
+    n_chains, L, G, A = 300, 16, 8, 0.2
+    k = 3.0 / (2 * 0.49)
+    types = [0] * 8 + [1] * 8
+    spec = _spec(2, (G, G, G), (float(G),) * 3, [Arch(L, n_chains, types, [[j, j + 1] for j in range(L - 1)],
+                                                     0.7 / np.sqrt(3.0))],
+                 xn=interaction_matrix(2, 0.0, 0.0), nref=L, k=k, A=A)
+    o = OracleSystem(spec)
+    o.init_coords()
+    x0 = o.coords().copy()
+    prof = np.where(np.arange(G) % 2 == 0, 0.5, -0.5)                    # omega_A by x; exact in FP32
+    w_a = np.broadcast_to(prof[None, None, :], (G, G, G)).reshape(-1)     # [z][y][x]
+    w32 = np.concatenate([w_a, -w_a]).astype(np.float32)
+    w64 = w32.astype(np.float64)
+    t32 = np.ascontiguousarray(types, dtype=np.int32)
+    pos = np.ascontiguousarray(x0.reshape(-1), dtype=np.float32)
+    burn, blocks, per = 400, 30, 20
+
+    def ref_run(n, seed):
+        return ref.rh_sweeps(n_chains, L, _p(t32, C.c_int), _p(pos, C.c_float), n, k, A, float(G), float(G),
+                             float(G), G, G, G, 2, _p(w64, C.c_double), seed)
+
+    ref_run(burn, 1)
+    r_acc, r_b2, r_fav = _sweep_statistics(lambda b: (ref_run(per, 100 + b), pos), n_chains, L, blocks, per)
+
+    def oracle_stats(fault):
+        orc = OracleSystem(spec)
+        orc.set_coords(x0)
+        orc.set_omega(w32)
+        orc.set_fault(fault)
+        orc.smc_move(burn)
+
+        def run(_):
+            a0 = orc.stats()["total_accepts"]
+            orc.smc_move(per)
+            return orc.stats()["total_accepts"] - a0, orc.coords()
+        return _sweep_statistics(run, n_chains, L, blocks, per)
+
+    def se(x):
+        return x.std(axis=0) / np.sqrt(len(x))
+
+    o_acc, o_b2, o_fav = oracle_stats(False)
+    assert 0.05 < r_acc.mean() < 0.5   # moves are accepted often enough to equilibrate
+    assert r_fav.mean() > 0.7          # the field does sort the beads
+    for what, r, q in (("acceptance", r_acc, o_acc), ("bond length", r_b2, o_b2), ("favoured", r_fav, o_fav)):
+        tol = 5 * np.hypot(se(r), se(q))
+        assert abs(r.mean() - q.mean()) < tol, (what, r.mean(), q.mean(), tol)
+
+    f_acc, f_b2, _ = oracle_stats(True)
+    assert abs(r_b2.mean() - f_b2.mean()) > 10 * np.hypot(se(r_b2), se(f_b2))
