@@ -214,6 +214,10 @@ def test_bench_reference_arm_contract():
     assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    # the same workload config as the GPU arm prints (bench.workload_config of the large system)
+    import bench
+    from new_arch_b200.spec import large_system
+    assert d["config"] == bench.workload_config(large_system(seed=7))
     env = dict(os.environ, RANK="1", WORLD_SIZE="2")
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
                        capture_output=True, text=True, timeout=120, cwd=ROOT, env=env)

@@ -285,4 +285,6 @@ def test_bench_line_contract():
     assert rf["bound"] == "hbm" and rf["unit"] == "GB/s" and 0 < rf["frac"] < 1.5
     assert abs(rf["frac"] - rf["achieved"] / rf["peak"]) < 1e-9
     assert d["e2e"]["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] > 0 and d["e2e"]["d2h_bytes_per_step"] > 0
-    assert "workload" in d["config"]
+    import bench
+    from new_arch_b200.spec import large_system
+    assert d["config"] == bench.workload_config(large_system(seed=7))   # what the reference arm prints
